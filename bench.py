@@ -1,0 +1,402 @@
+"""Benchmark: mode-n sparse MTTKRP with the device remap on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (default): the skewed 3-mode MTTKRP tensor -- dims 1,000,000 x
+200,000 x 50,000, 100M Zipf(s=1.1) coordinate draws per mode over a
+seed-permuted index set, duplicates merged (~64.7M nonzeros), LogNormal(0,1)
+values, rank 32 -- generated from a fixed seed (synthetic data, no files).
+
+One step = one full MTTKRP sweep (modes 0,1,2 in order; each mode computes
+Yhat[n] and remaps the slab for the next mode on the device).  `value` is
+GNNZ/s in the reference's convention nnz / t_sweep (src/main.cpp:970-972),
+over all ranks; `per_mode_gnnz_s` is nnz / t_mode.  Inputs stay resident
+(the slab is 1 GB, far larger than the 126 MB L2, so no L2 flush is needed).
+
+`e2e` is the same metric through the public host API
+(dgpu_mttkrp_sweep_host): every step uploads the factor matrices from pinned
+host memory, runs the sweep and downloads every Yhat.
+
+Multi-GPU: replicas only (each rank runs its own copy of the workload, no
+collective on the data path); value = total nnz processed / max-over-ranks
+time, scaling "weak".
+
+--impl reference times the reference's own CPU implementation (the
+reference sources compiled into oracle/_ref) on this host's cores, on the
+same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (1_000_000, 200_000, 50_000)
+DRAWS = 100_000_000
+ZIPF_S = 1.1
+SEED = 2
+RANK = 32
+METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--threads", type=int, default=8, help="plan worker count (FLYCOO geometry)")
+    ap.add_argument("--layout", default="pingpong", choices=["pingpong", "ncopy"])
+    ap.add_argument("--fiber", type=int, default=1)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--draws", type=int, default=DRAWS)
+    ap.add_argument("--rank", type=int, default=RANK)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=8_000_000,
+                    help="nonzeros in the CPU-baseline sample")
+    ap.add_argument("--cpals-iters", type=int, default=5)
+    ap.add_argument("--json-out", default=None)
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(args, device="cuda"):
+    from dynasor_plus_b200 import synth
+    if device == "cuda":
+        return synth.zipf_torch(DIMS, args.draws, ZIPF_S, SEED, device="cuda")
+    return synth.zipf(DIMS, args.draws, ZIPF_S, SEED)
+
+
+def uniform_factors(dims, R, seed=42):
+    rng = np.random.default_rng(seed)
+    Rp = (R + 15) // 16 * 16
+    Y = []
+    for d in dims:
+        y = np.zeros((int(d), Rp), np.float32)
+        y[:, :R] = rng.random((int(d), R), dtype=np.float32)
+        Y.append(y)
+    return Y
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+#  reference arm / CPU baseline
+# ---------------------------------------------------------------------------
+def reference_sweeps(dims, vals, idx, threads, R, warmup, steps, fiber_off=False, layout="pingpong"):
+    from oracle import bindings as B
+    ref = B.Reference(dims, vals, idx)
+    ref.build(threads, layout)
+    ref.factors(R)
+    Y = uniform_factors(dims, R)
+    for n in range(len(dims)):
+        ref.set_Y(n, Y[n])
+    ref.sweep_begin(fiber_off=fiber_off)
+    times = []
+    for s in range(warmup + steps):
+        t = 0.0
+        for n in range(len(dims)):
+            t += ref.process(n)
+        if s >= warmup:
+            times.append(t)
+    return times
+
+
+def subsample(dims, vals, idx, k, seed=5):
+    if k >= len(vals):
+        return dims, vals, idx
+    rng = np.random.default_rng(seed)
+    sel = np.sort(rng.choice(len(vals), k, replace=False))
+    return dims, vals[sel], [i[sel] for i in idx]
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from oracle import bindings as B
+    if not B.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref was not built (the reference tree was absent at build time)"}))
+        return
+    try:
+        dims, vals, idx = make_workload(args, "cuda")
+    except Exception:
+        dims, vals, idx = make_workload(args, "cpu")
+    cores = os.cpu_count() or 1
+    # bounded sample so W+K sweeps finish in a few minutes on any host
+    d2, v2, i2 = subsample(dims, vals, idx, min(len(vals), 16_000_000))
+    times = reference_sweeps(d2, v2, i2, cores, args.rank, args.warmup, args.steps)
+    t = statistics.median(times)
+    nnz = len(v2)
+    val = nnz / t / 1e9
+    out = {
+        "metric": METRIC, "value": val, "unit": "GNNZ/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "zipf1.1 3-mode 1000000x200000x50000, 100M draws deduped, rank 32",
+                   "sample_nnz": nnz, "full_nnz": len(vals), "layout": "pingpong",
+                   "threads": cores, "fiber": "reference default"},
+        "cpu_baseline": {"value": val, "unit": "GNNZ/s", "cores": cores, "kind": "reference",
+                         "sample": f"random {nnz} of {len(vals)} nonzeros, same dims"},
+        "e2e": {"value": val, "unit": "GNNZ/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------
+#  B200 arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+    import dynasor_plus_b200 as d
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    dims, vals, idx = make_workload(args, "cuda")
+    nnz = len(vals)
+    N = len(dims)
+    t0 = time.time()
+    plan = d.Plan(dims, vals, idx, threads=args.threads, rank=args.rank, layout=args.layout,
+                  fiber=bool(args.fiber), precision=args.precision, device=local)
+    build_s = time.time() - t0
+    stream = torch.cuda.Stream(device=local)
+    plan.set_stream(stream)
+    Y = uniform_factors(dims, args.rank)
+    for n in range(N):
+        plan.set_factor(n, Y[n])
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        plan.sweep()
+    plan.sync()
+
+    clk = ClockSampler(local)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.sweep()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = ws * nnz / (ms_step * 1e-3) / 1e9
+
+    # per-kernel timing pass (outside the timed region)
+    plan.set_timing(True)
+    plan.timing(reset=True)
+    for _ in range(2):
+        plan.sweep()
+    tim = plan.timing(reset=True)
+    plan.set_timing(False)
+    launches_per_step = sum(v["launches"] for v in tim.values()) // 2
+
+    # e2e through the host API with pinned buffers
+    Rp = plan.Rp
+    Yp = [torch.from_numpy(y).pin_memory() for y in Y]
+    Op = [torch.empty((int(dims[n]), Rp), dtype=torch.float32).pin_memory() for n in range(N)]
+    import ctypes as C
+    Yptr = (C.c_void_p * N)(*[t.data_ptr() for t in Yp])
+    Optr = (C.c_void_p * N)(*[t.data_ptr() for t in Op])
+    L = d.lib()
+    secs = C.c_double(0)
+    for _ in range(max(1, args.warmup)):
+        d.check(L.dgpu_mttkrp_sweep_host(plan._h, Yptr, Optr, C.byref(secs)))
+    barrier()
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.steps):
+        d.check(L.dgpu_mttkrp_sweep_host(plan._h, Yptr, Optr, C.byref(secs)))
+    a1.record(stream)
+    a1.synchronize()
+    e2e_ms = a0.elapsed_time(a1) / args.steps
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    fbytes = sum(int(dims[n]) * Rp * 4 for n in range(N))
+
+    # roofline of the dominant kernel (largest device-time share)
+    peak, peak_src = peaks()
+    dom = max(tim, key=lambda k: tim[k]["total_ms"])
+    dk = tim[dom]
+    dom_ms = dk["total_ms"] / max(1, dk["launches"])
+    dom_bytes = dk["bytes"] / max(1, dk["launches"])
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    total_ms = sum(v["total_ms"] for v in tim.values())
+    sweep_bytes = sum(v["bytes"] for v in tim.values()) / 2
+    # the north-star algorithmic bytes of a sweep with remap: per mode the
+    # slab read + the remap write + other factors once + Yhat once
+    R = args.rank
+    algo = 0.0
+    for n in range(N):
+        algo += 2 * nnz * (4 + 4 * N) + int(dims[n]) * R * 4
+        algo += sum(int(dims[w]) * R * (2 if args.precision == "bf16" else 4) for w in range(N) if w != n)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "GNNZ/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "bf16-gather/f32-acc",
+        "data": "synthetic",
+        "config": {"workload": f"zipf{ZIPF_S} 3-mode {DIMS[0]}x{DIMS[1]}x{DIMS[2]}, {args.draws} draws "
+                               f"deduped to {nnz} nnz, rank {args.rank}",
+                   "nnz": nnz, "layout": args.layout, "threads": args.threads,
+                   "fiber": bool(args.fiber), "precision": args.precision,
+                   "l2": "inputs larger than L2 (slab %.2f GB)" % (nnz * (4 + 4 * N) / 1e9),
+                   "parallelism": f"replicas x{ws}", "plan_build_s": round(build_s, 3)},
+        "per_mode_gnnz_s": ws * nnz * N / (ms_step * 1e-3) / 1e9,
+        "sweep_roofline": {"algorithmic_bytes": algo, "achieved_gbs": algo / (ms_step * 1e-3) / 1e9,
+                           "peak_gbs": peak, "frac": algo / (ms_step * 1e-3) / 1e9 / peak,
+                           "peak_source": peak_src},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_src, "avg_launch_ms": dom_ms,
+                     "algorithmic_bytes_per_launch": dom_bytes},
+        "kernel_times_ms_per_step": {k: v["total_ms"] / 2 for k, v in tim.items() if v["launches"]},
+        "kernel_share": {k: v["total_ms"] / total_ms for k, v in tim.items() if v["launches"]},
+        "gpu_launches": launches_per_step * args.steps,
+        "e2e": {"value": ws * nnz / (e2e_ms * 1e-3) / 1e9, "unit": "GNNZ/s",
+                "h2d_bytes_per_step": fbytes, "d2h_bytes_per_step": fbytes,
+                "ms_per_step": e2e_ms},
+        "clocks": clocks,
+    }
+
+    # CP-ALS iterations/s on the same tensor (Gauss-Seidel, FP64 solve)
+    if args.cpals_iters > 0:
+        r = plan.cpals(max_iters=args.cpals_iters, tol=0.0, seed=42)
+        out["cpals"] = {"iters": r["iters_done"], "iter_per_s": r["iters_done"] / r["total_time_s"],
+                        "final_fit": r["final_fit"], "mttkrp_s": r["mttkrp_time_s"],
+                        "linalg_s": r["linalg_time_s"]}
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import bindings as B
+            if B.ref_available():
+                d2, v2, i2 = subsample(dims, vals, idx, args.cpu_sample)
+                cores = os.cpu_count() or 1
+                times = reference_sweeps(d2, v2, i2, cores, args.rank, 1, 2)
+                t = statistics.median(times)
+                out["cpu_baseline"] = {"value": len(v2) / t / 1e9, "unit": "GNNZ/s", "cores": cores,
+                                       "kind": "reference",
+                                       "sample": f"random {len(v2)} of {nnz} nonzeros, same dims, "
+                                                 f"PingPong layout, --threads {cores}"}
+        except Exception as ex:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+
+    plan.close()
+    if rank == 0:
+        s = json.dumps(out)
+        print(s)
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                f.write(s + "\n")
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

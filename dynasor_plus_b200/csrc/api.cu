@@ -1,0 +1,386 @@
+// ============================================================================
+//  api.cu -- the extern "C" boundary of libdynasor_b200.so.
+//
+//  Every entry point validates its arguments, returns a DGPU_* status and
+//  records a one-line message for dgpu_last_error().  No exit(), no
+//  exceptions across the boundary.
+// ============================================================================
+#include "dgpu_internal.h"
+
+#include <chrono>
+#include <cstring>
+#include <new>
+
+namespace dgpu {
+int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o);
+int mode_pingpong(Plan& p, int n);
+int mode_ncopy(Plan& p, int n);
+int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& r, double* fit_history);
+}  // namespace dgpu
+
+using namespace dgpu;
+
+#define API_GUARD(p)                                                           \
+    do {                                                                       \
+        if (!(p)) {                                                            \
+            set_error("%s: null plan", __func__);                              \
+            return DGPU_ERR_ARG;                                               \
+        }                                                                      \
+        cudaError_t e_ = cudaSetDevice((p)->device);                           \
+        if (e_ != cudaSuccess) {                                               \
+            set_error("%s: cudaSetDevice: %s", __func__, cudaGetErrorString(e_)); \
+            return DGPU_ERR_CUDA;                                              \
+        }                                                                      \
+    } while (0)
+
+#define MODE_GUARD(p, n)                                                       \
+    do {                                                                       \
+        if ((n) < 0 || (n) >= (p)->N) {                                        \
+            set_error("%s: mode %d out of range [0,%d)", __func__, (n), (p)->N); \
+            return DGPU_ERR_ARG;                                               \
+        }                                                                      \
+    } while (0)
+
+extern "C" {
+
+const char* dgpu_last_error(void) { return last_error(); }
+
+int dgpu_version(void) { return 0x000100; }
+
+int dgpu_device_count(int* count) {
+    if (!count) { set_error("dgpu_device_count: null"); return DGPU_ERR_ARG; }
+    *count = 0;
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        set_error("cudaGetDeviceCount: %s", cudaGetErrorString(e));
+        return DGPU_ERR_CUDA;
+    }
+    return DGPU_OK;
+}
+
+void dgpu_plan_opts_default(dgpu_plan_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->threads = 1;
+    o->rank = 16;
+    o->layout = DGPU_LAYOUT_PINGPONG;
+    o->fiber = 1;
+    o->precision = DGPU_PREC_FP32;
+    o->device = 0;
+    o->mn_target = nullptr;
+}
+
+int dgpu_plan_create(const dgpu_tensor_desc* t, const dgpu_plan_opts* o, dgpu_plan** out) {
+    if (!t || !o || !out) { set_error("dgpu_plan_create: null argument"); return DGPU_ERR_ARG; }
+    *out = nullptr;
+    if (t->num_modes < 2 || t->num_modes > DGPU_MAX_MODES) {
+        set_error("dgpu_plan_create: num_modes %d outside [2,%d]", t->num_modes, DGPU_MAX_MODES);
+        return t->num_modes <= 0 ? DGPU_ERR_EMPTY : DGPU_ERR_ARG;
+    }
+    if (t->nnz == 0) { set_error("dgpu_plan_create: empty tensor (nnz = 0)"); return DGPU_ERR_EMPTY; }
+    if (t->nnz >= 0xffffffffull) {
+        set_error("dgpu_plan_create: nnz %llu exceeds the 32-bit slab positions",
+                  (unsigned long long)t->nnz);
+        return DGPU_ERR_ARG;
+    }
+    if (!t->mode_size || !t->vals || !t->idx) {
+        set_error("dgpu_plan_create: null tensor array"); return DGPU_ERR_ARG;
+    }
+    for (int n = 0; n < t->num_modes; ++n) {
+        if (!t->idx[n]) { set_error("dgpu_plan_create: idx[%d] is null", n); return DGPU_ERR_ARG; }
+        if (t->mode_size[n] == 0) {
+            set_error("dgpu_plan_create: mode %d has size 0", n); return DGPU_ERR_ARG;
+        }
+    }
+    if (o->threads < 1) { set_error("dgpu_plan_create: threads %d < 1", o->threads); return DGPU_ERR_ARG; }
+    if (o->rank < 1 || o->rank > 1024) {
+        set_error("dgpu_plan_create: rank %d outside [1,1024]", o->rank); return DGPU_ERR_ARG;
+    }
+    if (o->layout != DGPU_LAYOUT_PINGPONG && o->layout != DGPU_LAYOUT_NCOPY) {
+        set_error("dgpu_plan_create: unknown layout %d", o->layout); return DGPU_ERR_ARG;
+    }
+    if (o->precision != DGPU_PREC_FP32 && o->precision != DGPU_PREC_BF16) {
+        set_error("dgpu_plan_create: unknown precision %d", o->precision); return DGPU_ERR_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error("dgpu_plan_create: no CUDA device available");
+        return DGPU_ERR_CUDA;
+    }
+    if (o->device < 0 || o->device >= ndev) {
+        set_error("dgpu_plan_create: device %d outside [0,%d)", o->device, ndev);
+        return DGPU_ERR_ARG;
+    }
+    Plan* p = new (std::nothrow) Plan();
+    if (!p) { set_error("dgpu_plan_create: host OOM"); return DGPU_ERR_NOMEM; }
+    const int rc = plan_build(*p, *t, *o);
+    if (rc != DGPU_OK) {
+        delete p;
+        return rc;
+    }
+    *out = reinterpret_cast<dgpu_plan*>(p);
+    return DGPU_OK;
+}
+
+int dgpu_plan_destroy(dgpu_plan* plan) {
+    if (!plan) return DGPU_OK;
+    delete reinterpret_cast<Plan*>(plan);
+    return DGPU_OK;
+}
+
+int dgpu_plan_get_info(const dgpu_plan* plan, dgpu_plan_info* info) {
+    const Plan* p = reinterpret_cast<const Plan*>(plan);
+    if (!p || !info) { set_error("dgpu_plan_get_info: null argument"); return DGPU_ERR_ARG; }
+    std::memset(info, 0, sizeof(*info));
+    info->num_modes = p->N;
+    info->nnz = p->nnz;
+    info->rank = p->R;
+    info->rank_padded = p->Rp;
+    info->threads = p->T;
+    for (int n = 0; n < p->N; ++n) {
+        info->mode_size[n] = p->dims[n];
+        info->mn[n] = p->mn[n];
+        info->mn_shift[n] = p->shift[n];
+        info->shards_per_mode[n] = p->K[n];
+        info->kernel_class[n] = p->kclass[n];
+        info->avg_fiber_len[n] = p->afl[n];
+        info->tiles[n] = (uint32_t)p->tiles_h[n].size();
+    }
+    info->next_mode = p->next_mode;
+    info->device_bytes = p->device_bytes;
+    return DGPU_OK;
+}
+
+int dgpu_plan_set_stream(dgpu_plan* plan, void* stream) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    if (p->own_stream) cudaStreamDestroy(p->stream);
+    p->own_stream = false;
+    p->stream = static_cast<cudaStream_t>(stream);
+    return DGPU_OK;
+}
+
+int dgpu_plan_sync(dgpu_plan* plan) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    return DGPU_OK;
+}
+
+int dgpu_plan_set_timing(dgpu_plan* plan, int enable) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    DGPU_TRY(timing_collect(*p));
+    p->timing = enable != 0;
+    return DGPU_OK;
+}
+
+int dgpu_plan_get_timing(dgpu_plan* plan, dgpu_kernel_timing* out, int max, int* count,
+                         int reset) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (!count || (max > 0 && !out)) { set_error("dgpu_plan_get_timing: null"); return DGPU_ERR_ARG; }
+    DGPU_TRY(timing_collect(*p));
+    static const char* names[KK_COUNT] = {"mttkrp", "part_hist", "part_scan", "part_scatter",
+                                          "zero", "linalg"};
+    int k = 0;
+    for (int i = 0; i < KK_COUNT && k < max; ++i) {
+        std::memset(&out[k], 0, sizeof(out[k]));
+        std::strncpy(out[k].name, names[i], sizeof(out[k].name) - 1);
+        out[k].launches = p->t_launches[i];
+        out[k].total_ms = p->t_ms[i];
+        out[k].bytes = p->t_bytes[i];
+        ++k;
+    }
+    *count = k;
+    if (reset)
+        for (int i = 0; i < KK_COUNT; ++i) p->t_ms[i] = p->t_bytes[i] = 0, p->t_launches[i] = 0;
+    return DGPU_OK;
+}
+
+int dgpu_plan_shards(const dgpu_plan* plan, int n, uint64_t* begin, uint64_t* end) {
+    const Plan* p = reinterpret_cast<const Plan*>(plan);
+    if (!p || !begin || !end) { set_error("dgpu_plan_shards: null argument"); return DGPU_ERR_ARG; }
+    MODE_GUARD(p, n);
+    std::memcpy(begin, p->sbeg[n].data(), p->K[n] * sizeof(uint64_t));
+    std::memcpy(end, p->send[n].data(), p->K[n] * sizeof(uint64_t));
+    return DGPU_OK;
+}
+
+int dgpu_plan_schedule(const dgpu_plan* plan, int n, uint32_t* counts, uint32_t* flat,
+                       uint32_t* n_listed) {
+    const Plan* p = reinterpret_cast<const Plan*>(plan);
+    if (!p || !counts || !flat || !n_listed) {
+        set_error("dgpu_plan_schedule: null argument"); return DGPU_ERR_ARG;
+    }
+    MODE_GUARD(p, n);
+    uint32_t k = 0;
+    for (int t = 0; t < p->T; ++t) {
+        counts[t] = (uint32_t)p->sched[n][t].size();
+        for (uint32_t s : p->sched[n][t]) flat[k++] = s;
+    }
+    *n_listed = k;
+    return DGPU_OK;
+}
+
+int dgpu_upload_factor(dgpu_plan* plan, int n, const float* Y) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    MODE_GUARD(p, n);
+    if (!Y) { set_error("dgpu_upload_factor: null"); return DGPU_ERR_ARG; }
+    DGPU_CUDA(cudaMemcpyAsync(p->Y[n], Y, (size_t)p->dims[n] * p->Rp * sizeof(float),
+                              cudaMemcpyHostToDevice, p->stream));
+    p->yb_stale[n] = true;
+    return DGPU_OK;
+}
+
+int dgpu_download_factor(dgpu_plan* plan, int n, float* Y) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    MODE_GUARD(p, n);
+    if (!Y) { set_error("dgpu_download_factor: null"); return DGPU_ERR_ARG; }
+    DGPU_CUDA(cudaMemcpyAsync(Y, p->Y[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
+                              cudaMemcpyDeviceToHost, p->stream));
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    return DGPU_OK;
+}
+
+int dgpu_download_yhat(dgpu_plan* plan, int n, float* Yhat) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    MODE_GUARD(p, n);
+    if (!Yhat) { set_error("dgpu_download_yhat: null"); return DGPU_ERR_ARG; }
+    DGPU_CUDA(cudaMemcpyAsync(Yhat, p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
+                              cudaMemcpyDeviceToHost, p->stream));
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    return DGPU_OK;
+}
+
+int dgpu_download_lambda(dgpu_plan* plan, float* lambda) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (!lambda) { set_error("dgpu_download_lambda: null"); return DGPU_ERR_ARG; }
+    DGPU_CUDA(cudaMemcpyAsync(lambda, p->lambda, (size_t)p->R * sizeof(float),
+                              cudaMemcpyDeviceToHost, p->stream));
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    return DGPU_OK;
+}
+
+int dgpu_factor_device_ptr(dgpu_plan* plan, int n, void** Y, void** Yhat) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    if (!p) { set_error("dgpu_factor_device_ptr: null plan"); return DGPU_ERR_ARG; }
+    MODE_GUARD(p, n);
+    if (Y) *Y = p->Y[n];
+    if (Yhat) *Yhat = p->Yhat[n];
+    p->yb_stale[n] = true;   // the caller may write Y[n] directly
+    return DGPU_OK;
+}
+
+int dgpu_mttkrp_mode(dgpu_plan* plan, int n) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    MODE_GUARD(p, n);
+    if (p->layout == DGPU_LAYOUT_NCOPY) return mode_ncopy(*p, n);
+    return mode_pingpong(*p, n);
+}
+
+int dgpu_mttkrp_sweep(dgpu_plan* plan) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    for (int n = 0; n < p->N; ++n) {
+        const int rc = (p->layout == DGPU_LAYOUT_NCOPY) ? mode_ncopy(*p, n) : mode_pingpong(*p, n);
+        if (rc != DGPU_OK) return rc;
+    }
+    return DGPU_OK;
+}
+
+int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y, float* const* Yhat,
+                           double* secs) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (!Y || !Yhat) { set_error("dgpu_mttkrp_sweep_host: null"); return DGPU_ERR_ARG; }
+    for (int n = 0; n < p->N; ++n) DGPU_TRY(dgpu_upload_factor(plan, n, Y[n]));
+    cudaEvent_t e0, e1;
+    DGPU_CUDA(cudaEventCreate(&e0));
+    DGPU_CUDA(cudaEventCreate(&e1));
+    DGPU_CUDA(cudaEventRecord(e0, p->stream));
+    int rc = dgpu_mttkrp_sweep(plan);
+    if (rc == DGPU_OK) {
+        DGPU_CUDA(cudaEventRecord(e1, p->stream));
+        for (int n = 0; n < p->N && rc == DGPU_OK; ++n)
+            rc = (cudaMemcpyAsync(Yhat[n], p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
+                                  cudaMemcpyDeviceToHost, p->stream) == cudaSuccess)
+                     ? DGPU_OK : DGPU_ERR_CUDA;
+        cudaError_t e = cudaStreamSynchronize(p->stream);
+        if (e != cudaSuccess) {
+            set_error("dgpu_mttkrp_sweep_host: %s", cudaGetErrorString(e));
+            rc = DGPU_ERR_CUDA;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (secs) *secs = ms * 1e-3;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+int dgpu_download_slab(dgpu_plan* plan, float* vals, uint32_t* const* idx) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (!vals || !idx) { set_error("dgpu_download_slab: null"); return DGPU_ERR_ARG; }
+    const Slab& s = (p->layout == DGPU_LAYOUT_NCOPY) ? p->slab[p->next_mode] : p->slab[p->cur];
+    DGPU_CUDA(cudaMemcpyAsync(vals, s.vals, p->nnz * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    for (int n = 0; n < p->N; ++n) {
+        if (!idx[n]) { set_error("dgpu_download_slab: idx[%d] null", n); return DGPU_ERR_ARG; }
+        DGPU_CUDA(cudaMemcpyAsync(idx[n], s.idx[n], p->nnz * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, p->stream));
+    }
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    return DGPU_OK;
+}
+
+int dgpu_download_copy(dgpu_plan* plan, int k, float* vals, uint32_t* const* idx) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    MODE_GUARD(p, k);
+    if (p->layout != DGPU_LAYOUT_NCOPY) {
+        set_error("dgpu_download_copy: plan layout is not NCopy"); return DGPU_ERR_NOT_BUILT;
+    }
+    if (!vals || !idx) { set_error("dgpu_download_copy: null"); return DGPU_ERR_ARG; }
+    const Slab& s = p->slab[k];
+    DGPU_CUDA(cudaMemcpyAsync(vals, s.vals, p->nnz * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
+    for (int n = 0; n < p->N; ++n)
+        DGPU_CUDA(cudaMemcpyAsync(idx[n], s.idx[n], p->nnz * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, p->stream));
+    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    return DGPU_OK;
+}
+
+void dgpu_cp_options_default(dgpu_cp_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->max_iters = 50;
+    o->tol = 1e-4;
+    o->seed = 42;
+    o->ridge = 1e-10;
+    o->kernel = DGPU_CP_GAUSS_SEIDEL;
+    o->solve_fp64 = 1;
+    o->use_init = 0;
+    o->verbose = 0;
+}
+
+int dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt, dgpu_cp_result* res,
+               double* fit_history) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (!opt || !res) { set_error("dgpu_cpals: null argument"); return DGPU_ERR_ARG; }
+    if (opt->max_iters < 0) { set_error("dgpu_cpals: max_iters < 0"); return DGPU_ERR_ARG; }
+    return cpals_run(*p, *opt, *res, fit_history);
+}
+
+}  // extern "C"

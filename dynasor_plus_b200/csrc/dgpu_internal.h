@@ -1,0 +1,215 @@
+// ============================================================================
+//  dgpu_internal.h -- shared declarations of libdynasor_b200.so.
+//
+//  Device data layout of a plan (all in HBM):
+//
+//    slab[s]   s in {0,1} (PingPong) or {0..N-1} (NCopy):
+//              one cudaMalloc holding [vals f32 | idx[0] u32 | ... | idx[N-1]]
+//              each column 256 B aligned.  The SoA order matches the
+//              reference's Tensor (include/dynasor_common.h:345-352).
+//    Y[n], Yhat[n]      I_n x Rp FP32 row-major, padding columns zero.
+//    Yb[n]              I_n x Rp BF16 mirror of Y[n] for BF16 gathers.
+//    tiles[n]           work tiles of mode n in the reference's processing
+//                       order (LPT worker, shard list, slab position).
+//    part_cnt / part_off  per-(bucket, tile) counts and offsets of the
+//                       stable counting sort that implements the remap.
+// ============================================================================
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dynasor_b200.h"
+
+namespace dgpu {
+
+constexpr int kMaxModes = DGPU_MAX_MODES;
+
+// Elements per work tile (one CTA of the MTTKRP / partition kernels).
+constexpr uint32_t kTile = 4096;
+// Largest bucket count one partition pass handles; larger keys are split
+// into least-significant-digit passes of this many buckets.
+constexpr uint32_t kMaxBuckets = 2048;
+constexpr int kDigitBits = 11;   // log2(kMaxBuckets)
+
+// ----------------------------------------------------------------------------
+//  Error plumbing (thread-local last error, status codes, no exit()).
+// ----------------------------------------------------------------------------
+void set_error(const char* fmt, ...);
+const char* last_error();
+
+#define DGPU_CUDA(call)                                                        \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) {                                               \
+            ::dgpu::set_error("%s failed: %s (%s:%d)", #call,                  \
+                              cudaGetErrorString(e_), __FILE__, __LINE__);     \
+            return DGPU_ERR_CUDA;                                              \
+        }                                                                      \
+    } while (0)
+
+#define DGPU_TRY(expr)                                                         \
+    do {                                                                       \
+        int rc_ = (expr);                                                      \
+        if (rc_ != DGPU_OK) return rc_;                                        \
+    } while (0)
+
+// One work tile: `count` consecutive slab positions starting at `begin`,
+// all inside super-shard `shard` of the tile table's mode.
+struct Tile {
+    uint32_t begin;
+    uint32_t count;
+    uint32_t shard;
+    uint32_t pad;
+};
+
+// SoA slab on the device.
+struct Slab {
+    void*     raw = nullptr;
+    size_t    bytes = 0;
+    float*    vals = nullptr;
+    uint32_t* idx[kMaxModes] = {nullptr};
+};
+
+// Device pointer bundle passed by value to kernels.
+struct SlabPtrs {
+    const float*    vals;
+    const uint32_t* idx[kMaxModes];
+};
+struct SlabOut {
+    float*    vals;
+    uint32_t* idx[kMaxModes];
+};
+
+// Kernel classes tracked by the optional per-launch CUDA-event timer.
+enum KernelKind : int {
+    KK_MTTKRP = 0,       // mode-n MTTKRP
+    KK_PART_HIST = 1,    // partition: per-tile histograms
+    KK_PART_SCAN = 2,    // partition: exclusive scan
+    KK_PART_SCATTER = 3, // partition: stable scatter
+    KK_ZERO = 4,         // Yhat zeroing
+    KK_LINALG = 5,       // CP-ALS dense kernels
+    KK_COUNT = 6
+};
+
+struct TimedLaunch {
+    int         kind;
+    cudaEvent_t a, b;
+    double      bytes;    // algorithmic bytes of the launch
+};
+
+struct Plan {
+    // ---- per-launch timing (dgpu_plan_set_timing) -----------------------
+    bool                     timing = false;
+    std::vector<TimedLaunch> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double                   t_ms[KK_COUNT] = {};
+    double                   t_bytes[KK_COUNT] = {};
+    uint64_t                 t_launches[KK_COUNT] = {};
+
+    // ---- geometry ----------------------------------------------------
+    int       N = 0;
+    uint64_t  nnz = 0;
+    int       T = 1;
+    int       R = 0, Rp = 0;
+    int       layout = DGPU_LAYOUT_PINGPONG;
+    int       fiber = 1;
+    int       precision = DGPU_PREC_FP32;
+    int       device = 0;
+    uint32_t  dims[kMaxModes] = {};
+    uint32_t  mn[kMaxModes] = {};
+    int       shift[kMaxModes] = {};
+    uint32_t  K[kMaxModes] = {};
+    int       kclass[kMaxModes] = {};
+    double    afl[kMaxModes] = {};
+
+    // ---- host plan tables ---------------------------------------------
+    std::vector<std::vector<uint64_t>> count;   // [n][s]
+    std::vector<std::vector<uint64_t>> sbeg;    // [n][s]
+    std::vector<std::vector<uint64_t>> send;    // [n][s]
+    std::vector<std::vector<std::vector<uint32_t>>> sched;  // [n][tid]
+    std::vector<std::vector<Tile>> tiles_h;     // [n] processing order
+
+    // ---- device state -------------------------------------------------
+    cudaStream_t stream = nullptr;
+    bool         own_stream = false;
+    Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
+    int          cur = 0;                       // PingPong: live slab index
+    int          next_mode = 0;                 // PingPong: mode the slab is sorted for
+    Tile*        tiles_d[kMaxModes] = {nullptr};
+    Tile*        ident_tiles_d = nullptr;       // identity order over [0, nnz)
+    uint32_t     n_ident_tiles = 0;
+    float*       Y[kMaxModes] = {nullptr};
+    float*       Yhat[kMaxModes] = {nullptr};
+    __nv_bfloat16* Yb[kMaxModes] = {nullptr};
+    bool         yb_stale[kMaxModes] = {};
+    uint32_t*    part_cnt = nullptr;            // [buckets * tiles]
+    uint32_t*    part_off = nullptr;            // [buckets * tiles]
+    size_t       part_cap = 0;                  // entries
+    uint32_t*    scan_aux = nullptr;            // block sums for the scan
+    size_t       scan_aux_cap = 0;
+    int*         err_flag = nullptr;            // device-side fault flag
+    float*       lambda = nullptr;              // [Rp]
+    double*      la_work = nullptr;             // CP-ALS R x R scratch (FP64)
+    size_t       la_work_cap = 0;
+    float*       la_f32 = nullptr;              // FP32 scratch (Grams etc.)
+    size_t       la_f32_cap = 0;
+    uint64_t     device_bytes = 0;
+
+    ~Plan();
+};
+
+// ---- optional launch timing ------------------------------------------------
+// Brackets one launch with CUDA events on the plan stream when timing is on.
+struct LaunchTimer {
+    Plan&       p;
+    int         kind;
+    double      bytes;
+    cudaEvent_t a = nullptr;
+    LaunchTimer(Plan& pl, int k, double b);
+    ~LaunchTimer();
+};
+int timing_collect(Plan& p);
+
+// ---- device memory helpers ----------------------------------------------
+int  dev_alloc(Plan& p, void** ptr, size_t bytes);
+void dev_free(void* ptr);
+int  slab_alloc(Plan& p, Slab& s);
+SlabPtrs slab_in(const Slab& s, int N);
+SlabOut  slab_out(const Slab& s, int N);
+
+// ---- kernels launched from host code (defined in .cu files) -------------
+// Per-mode shard histograms of the input COO (flat, sum of K_n bins) and
+// an out-of-range index check.
+int launch_shard_counts(Plan& p, const Slab& s, uint64_t* counts_d, size_t total_bins);
+
+// Stable partition: the elements listed by `tiles` (processing order) are
+// written to `out` ordered by key = (idx[key_mode] >> key_shift) & key_mask
+// (buckets < nb <= kMaxBuckets), each bucket starting at `base_off` +
+// (elements of all smaller buckets), stably.  Uses p.part_cnt/part_off.
+int stable_partition(Plan& p, const Slab& in, const Tile* tiles, uint32_t ntiles,
+                     int key_mode, int key_shift, uint32_t key_mask, uint32_t nb,
+                     const Slab& out);
+// Stable sort of the sequence listed by `tiles` over slab[a] by the key
+// (idx[key_mode] >> key_shift) < key_limit, any key range: one partition
+// pass per least-significant digit, ping-ponging between slab[a] and
+// slab[b]; *result receives the slab index that holds the sorted data.
+int stable_sort_pingpong(Plan& p, int a, int b, const Tile* tiles, uint32_t ntiles,
+                         int key_mode, int key_shift, uint64_t key_limit, int* result);
+
+// MTTKRP of mode n over the tiles of the slab `in` into p.Yhat[n].
+int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles);
+int launch_mttkrp_all_modes(Plan& p, const Slab& in);
+
+// FP32 -> BF16 factor mirror.
+int launch_to_bf16(Plan& p, int n);
+
+// Dense CP-ALS pieces.
+int cp_tensor_norm(Plan& p, const float* vals, double* out);
+int launch_model_values(Plan& p, const Slab& in, float* out);
+int cpopt_gradient(Plan& p, float* const* grad_host);
+
+}  // namespace dgpu

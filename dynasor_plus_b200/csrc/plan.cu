@@ -1,0 +1,493 @@
+// ============================================================================
+//  plan.cu -- FLYCOO plan construction on the device (replaces the FLYCOO
+//  part of build_flycoo, src/dynasor_preprocess.cpp:2013-2163).
+//
+//    host    geometry: m_n = pick_mn(I_n, T), shift, K_n, kernel class
+//            [src/dynasor_preprocess.cpp:87-99, 2031-2048, 2087-2095]
+//    device  shard histogram of every mode + index range check
+//            [sort_and_count_all pass A, :153-174]
+//    host    greedy LPT schedule from the counts, shard_begin/end
+//            [:291-323, :363-384]; work tiles in processing order
+//    device  stable scatter into mode-0 shard order [pass B, :212-241]
+//    device  NCopy copies (remap chain + fiber sorts) when requested
+//            [:1740-1790]
+//
+//  The LPT step uses std::sort with the reference's comparator so ties
+//  resolve identically (libstdc++ introsort), and the same (load, tid)
+//  min-heap, which makes the processing order -- and therefore the remap
+//  permutation -- identical to the reference's for the same worker count.
+// ============================================================================
+#include "dgpu_internal.h"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <queue>
+
+namespace dgpu {
+
+int stable_sort_pingpong(Plan& p, int a, int b, const Tile* tiles, uint32_t ntiles,
+                         int key_mode, int key_shift, uint64_t key_limit, int* result);
+
+// ----------------------------------------------------------------------------
+//  errors
+// ----------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+const char* last_error() { return g_err; }
+
+// ----------------------------------------------------------------------------
+//  memory
+// ----------------------------------------------------------------------------
+int dev_alloc(Plan& p, void** ptr, size_t bytes) {
+    *ptr = nullptr;
+    if (bytes == 0) bytes = 256;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+        return DGPU_ERR_NOMEM;
+    }
+    p.device_bytes += bytes;
+    return DGPU_OK;
+}
+
+void dev_free(void* ptr) {
+    if (ptr) cudaFree(ptr);
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int slab_alloc(Plan& p, Slab& s) {
+    const size_t vb = align256(p.nnz * sizeof(float));
+    const size_t ib = align256(p.nnz * sizeof(uint32_t));
+    s.bytes = vb + (size_t)p.N * ib;
+    DGPU_TRY(dev_alloc(p, &s.raw, s.bytes));
+    char* c = static_cast<char*>(s.raw);
+    s.vals = reinterpret_cast<float*>(c);
+    c += vb;
+    for (int n = 0; n < p.N; ++n) {
+        s.idx[n] = reinterpret_cast<uint32_t*>(c);
+        c += ib;
+    }
+    return DGPU_OK;
+}
+
+SlabPtrs slab_in(const Slab& s, int N) {
+    SlabPtrs r{};
+    r.vals = s.vals;
+    for (int n = 0; n < N; ++n) r.idx[n] = s.idx[n];
+    return r;
+}
+SlabOut slab_out(const Slab& s, int N) {
+    SlabOut r{};
+    r.vals = s.vals;
+    for (int n = 0; n < N; ++n) r.idx[n] = s.idx[n];
+    return r;
+}
+
+// ----------------------------------------------------------------------------
+//  optional per-launch timing
+// ----------------------------------------------------------------------------
+static cudaEvent_t pool_get(Plan& p) {
+    if (!p.event_pool.empty()) {
+        cudaEvent_t e = p.event_pool.back();
+        p.event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+LaunchTimer::LaunchTimer(Plan& pl, int k, double b) : p(pl), kind(k), bytes(b) {
+    if (!p.timing) return;
+    a = pool_get(p);
+    if (a) cudaEventRecord(a, p.stream);
+}
+
+LaunchTimer::~LaunchTimer() {
+    if (!p.timing || !a) return;
+    cudaEvent_t b = pool_get(p);
+    if (!b) { p.event_pool.push_back(a); return; }
+    cudaEventRecord(b, p.stream);
+    p.pending.push_back({kind, a, b, bytes});
+    if (p.pending.size() > 4096) timing_collect(p);
+}
+
+int timing_collect(Plan& p) {
+    if (p.pending.empty()) return DGPU_OK;
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    for (auto& t : p.pending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t.a, t.b);
+        p.t_ms[t.kind] += ms;
+        p.t_bytes[t.kind] += t.bytes;
+        p.t_launches[t.kind] += 1;
+        p.event_pool.push_back(t.a);
+        p.event_pool.push_back(t.b);
+    }
+    p.pending.clear();
+    return DGPU_OK;
+}
+
+Plan::~Plan() {
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& t : pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    for (auto e : event_pool) cudaEventDestroy(e);
+    for (auto& s : slab) dev_free(s.raw);
+    for (int n = 0; n < kMaxModes; ++n) {
+        dev_free(tiles_d[n]);
+        dev_free(Y[n]);
+        dev_free(Yhat[n]);
+        dev_free(Yb[n]);
+    }
+    dev_free(ident_tiles_d);
+    dev_free(part_cnt);
+    dev_free(part_off);
+    dev_free(scan_aux);
+    dev_free(err_flag);
+    dev_free(lambda);
+    dev_free(la_work);
+    dev_free(la_f32);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+// ----------------------------------------------------------------------------
+//  geometry helpers (src/dynasor_preprocess.cpp:69-99)
+// ----------------------------------------------------------------------------
+static uint32_t round_up_pow2(uint32_t x) {
+    if (x <= 1) return 1;
+    uint32_t r = 1;
+    while (r < x) r <<= 1;
+    return r;
+}
+static int log2_ceil(uint32_t x) {
+    int k = 0;
+    while ((uint32_t(1) << k) < x) ++k;
+    return k;
+}
+static uint32_t rows_per_shard(uint32_t I, int T) {
+    if (I <= (uint32_t)T) return 1;
+    uint32_t mn = I / ((uint32_t)T * 4u);
+    mn = std::max(mn, 1u);
+    mn = std::max(mn, 16u);
+    mn = std::min(mn, 16384u);
+    if (mn > I) mn = I;
+    return round_up_pow2(mn);
+}
+
+// ----------------------------------------------------------------------------
+//  device: per-mode shard histograms + index range check
+// ----------------------------------------------------------------------------
+struct Geom {
+    uint32_t dims[kMaxModes];
+    int      shift[kMaxModes];
+    uint32_t binoff[kMaxModes];
+};
+
+__global__ void k_shard_counts(SlabPtrs in, int N, uint64_t nnz, Geom g, uint32_t total,
+                               int use_smem, unsigned long long* __restrict__ counts,
+                               int* __restrict__ err)
+{
+    extern __shared__ uint32_t h[];
+    if (use_smem) {
+        for (uint32_t b = threadIdx.x; b < total; b += blockDim.x) h[b] = 0;
+        __syncthreads();
+    }
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        for (int n = 0; n < N; ++n) {
+            const uint32_t r = in.idx[n][i];
+            if (r >= g.dims[n]) {
+                atomicExch(err, 1);
+                continue;
+            }
+            const uint32_t bin = g.binoff[n] + (r >> g.shift[n]);
+            if (use_smem) atomicAdd(&h[bin], 1u);
+            else atomicAdd(&counts[bin], 1ull);
+        }
+    }
+    if (use_smem) {
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < total; b += blockDim.x)
+            if (h[b]) atomicAdd(&counts[b], (unsigned long long)h[b]);
+    }
+}
+
+// ----------------------------------------------------------------------------
+//  host: LPT schedule and tiles
+// ----------------------------------------------------------------------------
+static void build_schedule(Plan& p) {
+    p.sched.assign(p.N, std::vector<std::vector<uint32_t>>(p.T));
+    for (int n = 0; n < p.N; ++n) {
+        const uint64_t* cn = p.count[n].data();
+        std::vector<uint32_t> order(p.K[n]);
+        std::iota(order.begin(), order.end(), 0u);
+        std::sort(order.begin(), order.end(),
+                  [&](uint32_t a, uint32_t b) { return cn[a] > cn[b]; });
+        using QE = std::pair<uint64_t, int>;
+        std::priority_queue<QE, std::vector<QE>, std::greater<QE>> heap;
+        for (int t = 0; t < p.T; ++t) heap.push({0ull, t});
+        for (uint32_t s : order) {
+            if (cn[s] == 0) continue;
+            const QE top = heap.top();
+            heap.pop();
+            p.sched[n][top.second].push_back(s);
+            heap.push({top.first + cn[s], top.second});
+        }
+    }
+}
+
+static void build_tiles(Plan& p) {
+    p.tiles_h.assign(p.N, {});
+    for (int n = 0; n < p.N; ++n) {
+        auto& v = p.tiles_h[n];
+        for (int t = 0; t < p.T; ++t)
+            for (uint32_t s : p.sched[n][t]) {
+                const uint64_t b = p.sbeg[n][s], e = p.send[n][s];
+                for (uint64_t x = b; x < e; x += kTile) {
+                    Tile tl;
+                    tl.begin = (uint32_t)x;
+                    tl.count = (uint32_t)std::min<uint64_t>(kTile, e - x);
+                    tl.shard = s;
+                    tl.pad = 0;
+                    v.push_back(tl);
+                }
+            }
+    }
+}
+
+static int upload_tiles(Plan& p, const std::vector<Tile>& h, Tile** d) {
+    DGPU_TRY(dev_alloc(p, (void**)d, std::max<size_t>(1, h.size()) * sizeof(Tile)));
+    if (!h.empty())
+        DGPU_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(Tile),
+                                  cudaMemcpyHostToDevice, p.stream));
+    return DGPU_OK;
+}
+
+// ----------------------------------------------------------------------------
+//  plan creation
+// ----------------------------------------------------------------------------
+int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
+    p.N = t.num_modes;
+    p.nnz = t.nnz;
+    p.T = o.threads;
+    p.R = o.rank;
+    p.Rp = (o.rank + 15) / 16 * 16;
+    p.layout = o.layout;
+    p.fiber = o.fiber ? 1 : 0;
+    p.precision = o.precision;
+    p.device = o.device;
+    DGPU_CUDA(cudaSetDevice(p.device));
+    if (!p.stream) {
+        DGPU_CUDA(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+        p.own_stream = true;
+    }
+
+    // geometry
+    for (int n = 0; n < p.N; ++n) {
+        p.dims[n] = t.mode_size[n];
+        uint32_t mn;
+        if (o.mn_target && o.mn_target[n] > 0) mn = round_up_pow2(o.mn_target[n]);
+        else mn = rows_per_shard(p.dims[n], p.T);
+        p.mn[n] = mn;
+        p.shift[n] = log2_ceil(mn);
+        p.K[n] = (p.dims[n] + mn - 1) / mn;
+        if (p.K[n] == 0) p.K[n] = 1;
+        p.afl[n] = (double)p.nnz / (double)std::max<uint32_t>(1u, p.dims[n]);
+        p.kclass[n] = p.afl[n] >= 32.0 ? 2 : (p.afl[n] >= 8.0 ? 1 : 0);
+    }
+
+    // slabs: PingPong keeps primary + scratch; NCopy keeps N copies (+1
+    // scratch while sorting).
+    const int nslab = (p.layout == DGPU_LAYOUT_NCOPY) ? std::max(p.N + 1, 2) : 2;
+    if (nslab > kMaxModes) {
+        set_error("NCopy with %d modes needs %d slabs (max %d)", p.N, nslab, kMaxModes);
+        return DGPU_ERR_ARG;
+    }
+    for (int s = 0; s < nslab; ++s) DGPU_TRY(slab_alloc(p, p.slab[s]));
+    DGPU_TRY(dev_alloc(p, (void**)&p.err_flag, sizeof(int)));
+    DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
+
+    // input COO -> slab[1] (the reference's loader order)
+    const int in_slab = 1;
+    DGPU_CUDA(cudaMemcpyAsync(p.slab[in_slab].vals, t.vals, p.nnz * sizeof(float),
+                              cudaMemcpyHostToDevice, p.stream));
+    for (int n = 0; n < p.N; ++n)
+        DGPU_CUDA(cudaMemcpyAsync(p.slab[in_slab].idx[n], t.idx[n], p.nnz * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice, p.stream));
+
+    // shard histograms on the device
+    Geom g{};
+    uint32_t total = 0;
+    for (int n = 0; n < p.N; ++n) {
+        g.dims[n] = p.dims[n];
+        g.shift[n] = p.shift[n];
+        g.binoff[n] = total;
+        total += p.K[n];
+    }
+    unsigned long long* counts_d = nullptr;
+    DGPU_TRY(dev_alloc(p, (void**)&counts_d, (size_t)total * 8));
+    DGPU_CUDA(cudaMemsetAsync(counts_d, 0, (size_t)total * 8, p.stream));
+    const int use_smem = total <= 12288 ? 1 : 0;
+    const unsigned blocks =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((p.nnz + 255) / 256, 148 * 8));
+    k_shard_counts<<<blocks, 256, use_smem ? total * 4 : 0, p.stream>>>(
+        slab_in(p.slab[in_slab], p.N), p.N, p.nnz, g, total, use_smem, counts_d, p.err_flag);
+    DGPU_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> counts_h(total);
+    int err_h = 0;
+    DGPU_CUDA(cudaMemcpyAsync(counts_h.data(), counts_d, (size_t)total * 8,
+                              cudaMemcpyDeviceToHost, p.stream));
+    DGPU_CUDA(cudaMemcpyAsync(&err_h, p.err_flag, sizeof(int), cudaMemcpyDeviceToHost, p.stream));
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    dev_free(counts_d);
+    p.device_bytes -= (size_t)total * 8;
+    if (err_h) {
+        set_error("plan: an index is out of range of its mode size");
+        return DGPU_ERR_INDEX;
+    }
+
+    p.count.assign(p.N, {});
+    p.sbeg.assign(p.N, {});
+    p.send.assign(p.N, {});
+    for (int n = 0; n < p.N; ++n) {
+        p.count[n].assign(counts_h.begin() + g.binoff[n], counts_h.begin() + g.binoff[n] + p.K[n]);
+        p.sbeg[n].resize(p.K[n]);
+        p.send[n].resize(p.K[n]);
+        uint64_t c = 0;
+        for (uint32_t s = 0; s < p.K[n]; ++s) {
+            p.sbeg[n][s] = c;
+            c += p.count[n][s];
+            p.send[n][s] = c;
+        }
+    }
+    build_schedule(p);
+    build_tiles(p);
+    for (int n = 0; n < p.N; ++n) DGPU_TRY(upload_tiles(p, p.tiles_h[n], &p.tiles_d[n]));
+    {
+        std::vector<Tile> id;
+        for (uint64_t x = 0; x < p.nnz; x += kTile) {
+            Tile tl;
+            tl.begin = (uint32_t)x;
+            tl.count = (uint32_t)std::min<uint64_t>(kTile, p.nnz - x);
+            tl.shard = 0;
+            tl.pad = 0;
+            id.push_back(tl);
+        }
+        p.n_ident_tiles = (uint32_t)id.size();
+        DGPU_TRY(upload_tiles(p, id, &p.ident_tiles_d));
+    }
+
+    // stable scatter of the input order into mode-0 shard order
+    int res = 0;
+    DGPU_TRY(stable_sort_pingpong(p, in_slab, 0, p.ident_tiles_d, p.n_ident_tiles, 0,
+                                  p.shift[0], p.K[0], &res));
+    p.cur = res;
+    p.next_mode = 0;
+
+    if (p.layout == DGPU_LAYOUT_NCOPY) {
+        // copy 0 lives in slab[0]; copy k = remap of copy k-1 by the mode
+        // (k-1) processing order, keyed by the mode-k shard.  The spare
+        // slab p.N is the LSD intermediate.
+        if (p.cur != 0) {
+            DGPU_CUDA(cudaMemcpyAsync(p.slab[0].raw, p.slab[p.cur].raw, p.slab[0].bytes,
+                                      cudaMemcpyDeviceToDevice, p.stream));
+        }
+        for (int k = 1; k < p.N; ++k) {
+            DGPU_CUDA(cudaMemcpyAsync(p.slab[k].raw, p.slab[k - 1].raw, p.slab[k].bytes,
+                                      cudaMemcpyDeviceToDevice, p.stream));
+            int r = 0;
+            DGPU_TRY(stable_sort_pingpong(p, k, p.N, p.tiles_d[k - 1],
+                                          (uint32_t)p.tiles_h[k - 1].size(), k, p.shift[k],
+                                          p.K[k], &r));
+            if (r != k)
+                DGPU_CUDA(cudaMemcpyAsync(p.slab[k].raw, p.slab[r].raw, p.slab[k].bytes,
+                                          cudaMemcpyDeviceToDevice, p.stream));
+        }
+        if (p.fiber) {
+            for (int k = 0; k < p.N; ++k) {
+                if (p.kclass[k] != 2) continue;
+                int r = 0;
+                DGPU_TRY(stable_sort_pingpong(p, k, p.N, p.ident_tiles_d, p.n_ident_tiles, k, 0,
+                                              p.dims[k], &r));
+                if (r != k)
+                    DGPU_CUDA(cudaMemcpyAsync(p.slab[k].raw, p.slab[r].raw, p.slab[k].bytes,
+                                              cudaMemcpyDeviceToDevice, p.stream));
+            }
+        }
+    }
+
+    // factors
+    for (int n = 0; n < p.N; ++n) {
+        const size_t fb = (size_t)p.dims[n] * p.Rp * sizeof(float);
+        DGPU_TRY(dev_alloc(p, (void**)&p.Y[n], fb));
+        DGPU_TRY(dev_alloc(p, (void**)&p.Yhat[n], fb));
+        DGPU_CUDA(cudaMemsetAsync(p.Y[n], 0, fb, p.stream));
+        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, fb, p.stream));
+        if (p.precision == DGPU_PREC_BF16) {
+            DGPU_TRY(dev_alloc(p, (void**)&p.Yb[n], fb / 2));
+            DGPU_CUDA(cudaMemsetAsync(p.Yb[n], 0, fb / 2, p.stream));
+        }
+        p.yb_stale[n] = true;
+    }
+    DGPU_TRY(dev_alloc(p, (void**)&p.lambda, (size_t)p.Rp * sizeof(float)));
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    return DGPU_OK;
+}
+
+// One mode of the PingPong sweep: fiber sort (DenseFiber modes), MTTKRP,
+// device remap for mode n+1.  src/dynasor.cpp:352-539.
+int mode_pingpong(Plan& p, int n) {
+    if (n != p.next_mode) {
+        set_error("mttkrp_mode(%d): the slab is remapped for mode %d; modes must run in "
+                  "order 0..N-1", n, p.next_mode);
+        return DGPU_ERR_ORDER;
+    }
+    const int other = 1 - p.cur;
+    if (p.fiber && p.kclass[n] == 2) {
+        int r = 0;
+        DGPU_TRY(stable_sort_pingpong(p, p.cur, other, p.ident_tiles_d, p.n_ident_tiles, n, 0,
+                                      p.dims[n], &r));
+        p.cur = r;
+    }
+    {
+        const size_t yb = (size_t)p.dims[n] * p.Rp * sizeof(float);
+        LaunchTimer t(p, KK_ZERO, (double)yb);
+        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, yb, p.stream));
+    }
+    DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
+    const int nm = (n + 1) % p.N;
+    int r = 0;
+    DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.tiles_d[n],
+                                  (uint32_t)p.tiles_h[n].size(), nm, p.shift[nm], p.K[nm], &r));
+    p.cur = r;
+    p.next_mode = nm;
+    return DGPU_OK;
+}
+
+int mode_ncopy(Plan& p, int n) {
+    {
+        const size_t yb = (size_t)p.dims[n] * p.Rp * sizeof(float);
+        LaunchTimer t(p, KK_ZERO, (double)yb);
+        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, yb, p.stream));
+    }
+    DGPU_TRY(launch_mttkrp(p, n, p.slab[n], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
+    p.next_mode = (n + 1) % p.N;
+    return DGPU_OK;
+}
+
+}  // namespace dgpu

@@ -1,0 +1,241 @@
+/* ==========================================================================
+ *  dynasor_b200.h -- C ABI of the B200 (sm_100a) sparse MTTKRP / CP-ALS
+ *  engine (libdynasor_b200.so).
+ *
+ *  Plain C: opaque handles, raw host pointers and sizes, integer status
+ *  codes.  No CUDA or torch types appear in any signature (CUDA streams are
+ *  passed as void*).  Every function returns DGPU_OK (0) or a negative
+ *  DGPU_ERR_* code; dgpu_last_error() gives a one-line description of the
+ *  most recent failure on the calling thread.  Nothing here calls exit().
+ *
+ *  Data conventions are the reference's (include/dynasor_common.h:28-30,
+ *  604-615, include/dynasor_linalg.h:8-17):
+ *    * indices are 0-based uint32, values float32, COO as SoA
+ *      (vals[nnz], idx[n][nnz]);
+ *    * factor matrices are row-major I_n x Rp float32 with
+ *      Rp = round_up(R, 16) and the padding columns zero;
+ *    * the FLYCOO plan depends on the worker count `threads` exactly as the
+ *      reference's plan depends on --threads, so a plan built here with
+ *      threads=T produces the same slab permutation as the reference built
+ *      with --threads T.
+ *
+ *  Threading: a plan is not thread-safe; all of its device work is issued
+ *  on one CUDA stream (its own, or one set with dgpu_plan_set_stream).
+ * ========================================================================== */
+#ifndef DYNASOR_B200_H
+#define DYNASOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGPU_MAX_MODES 8
+
+/* ---- status codes --------------------------------------------------- */
+#define DGPU_OK              0
+#define DGPU_ERR_ARG        -1   /* bad argument / unsupported shape      */
+#define DGPU_ERR_CUDA       -2   /* a CUDA runtime call failed            */
+#define DGPU_ERR_NOMEM      -3   /* device or host allocation failed      */
+#define DGPU_ERR_EMPTY      -4   /* tensor has no nonzeros / no modes     */
+#define DGPU_ERR_INDEX      -5   /* an index is >= its mode size          */
+#define DGPU_ERR_ORDER      -6   /* modes processed out of order          */
+#define DGPU_ERR_IO         -7   /* file missing, truncated or malformed  */
+#define DGPU_ERR_NOT_BUILT  -8   /* required plan state is missing        */
+#define DGPU_ERR_DEVICE     -9   /* a kernel reported an internal fault   */
+
+/* ---- layouts / kernels (values match the reference enums) ------------ */
+#define DGPU_LAYOUT_PINGPONG 0   /* Layout::PingPong: remap every mode    */
+#define DGPU_LAYOUT_NCOPY    1   /* Layout::NCopy: N pre-sorted copies    */
+
+#define DGPU_CP_GAUSS_SEIDEL 0   /* CpKernel::GaussSeidel                 */
+#define DGPU_CP_JACOBI       1   /* CpKernel::Jacobi (all-modes pass)     */
+
+#define DGPU_PREC_FP32       0   /* FP32 gathers, FP32 accumulation       */
+#define DGPU_PREC_BF16       1   /* BF16 gathers (FP32 master factors)    */
+
+typedef struct dgpu_plan dgpu_plan;   /* opaque */
+
+/* Host COO tensor description (0-based indices). */
+typedef struct {
+    int             num_modes;
+    uint64_t        nnz;
+    const uint32_t* mode_size;    /* [num_modes]                         */
+    const float*    vals;         /* [nnz]                               */
+    const uint32_t* const* idx;   /* [num_modes][nnz]                    */
+} dgpu_tensor_desc;
+
+/* Plan options. */
+typedef struct {
+    int       threads;            /* reference worker count (>= 1)       */
+    int       rank;               /* R (>= 1); Rp = round_up(R, 16)      */
+    int       layout;             /* DGPU_LAYOUT_*                       */
+    int       fiber;              /* 1: fiber-sort DenseFiber modes (the
+                                     reference default); 0: the layout of
+                                     DYN_FIBER_OFF=1                     */
+    int       precision;          /* DGPU_PREC_*                         */
+    int       device;             /* CUDA device ordinal                 */
+    const uint32_t* mn_target;    /* optional rows-per-shard override
+                                     (NULL = pick like pick_mn)          */
+} dgpu_plan_opts;
+
+/* Per-mode plan facts (mirrors Tensor fields, include/dynasor_common.h:322-343). */
+typedef struct {
+    int       num_modes;
+    uint64_t  nnz;
+    int       rank;
+    int       rank_padded;
+    int       threads;
+    uint32_t  mode_size[DGPU_MAX_MODES];
+    uint32_t  mn[DGPU_MAX_MODES];               /* rows per super-shard   */
+    int       mn_shift[DGPU_MAX_MODES];
+    uint32_t  shards_per_mode[DGPU_MAX_MODES];
+    int       kernel_class[DGPU_MAX_MODES];     /* 0 sparse,1 medium,2 dense */
+    double    avg_fiber_len[DGPU_MAX_MODES];
+    uint32_t  tiles[DGPU_MAX_MODES];            /* device work tiles      */
+    int       next_mode;                        /* mode the slab is ready for */
+    uint64_t  device_bytes;                     /* HBM held by the plan   */
+} dgpu_plan_info;
+
+/* CP-ALS options / result (mirror CpOptions / CpResult,
+ * include/dynasor_cpals.h:82-114). */
+typedef struct {
+    int       max_iters;          /* default 50                           */
+    double    tol;                /* stop when |fit_i - fit_{i-1}| < tol  */
+    uint64_t  seed;               /* N(0,1) init seed (default 42)        */
+    double    ridge;              /* relative ridge (default 1e-10)       */
+    int       kernel;             /* DGPU_CP_*                            */
+    int       solve_fp64;         /* 1: FP64 Cholesky + solve (default)   */
+    int       use_init;           /* 1: start from the uploaded factors   */
+    int       verbose;            /* print the reference's [cpals] lines  */
+} dgpu_cp_options;
+
+typedef struct {
+    int       iters_done;
+    double    final_fit;
+    double    final_residual;
+    double    tensor_norm;
+    double    total_time_s;
+    double    mttkrp_time_s;
+    double    linalg_time_s;
+} dgpu_cp_result;
+
+/* ---- errors ----------------------------------------------------------- */
+const char* dgpu_last_error(void);
+int         dgpu_version(void);                   /* 0xMMmmpp             */
+int         dgpu_device_count(int* count);
+
+/* ---- plan (replaces build_flycoo: src/dynasor_preprocess.cpp:2013-2163) */
+void dgpu_plan_opts_default(dgpu_plan_opts* opts);
+int  dgpu_plan_create(const dgpu_tensor_desc* tensor, const dgpu_plan_opts* opts,
+                      dgpu_plan** out);
+int  dgpu_plan_destroy(dgpu_plan* plan);
+int  dgpu_plan_get_info(const dgpu_plan* plan, dgpu_plan_info* info);
+int  dgpu_plan_set_stream(dgpu_plan* plan, void* cuda_stream);
+int  dgpu_plan_sync(dgpu_plan* plan);
+
+/* Per-launch device timing (the reference only times phases with
+ * omp_get_wtime, src/dynasor.cpp:393,538).  When enabled every kernel launch
+ * is bracketed by CUDA events on the plan stream; dgpu_plan_get_timing
+ * synchronises, folds the pending pairs into per-kind totals and copies
+ * up to `max` records.  Kinds: "mttkrp", "part_hist", "part_scan",
+ * "part_scatter", "zero", "linalg".  `bytes` is the algorithmic byte count
+ * (each input read once, each output written once) summed over launches. */
+typedef struct {
+    char      name[24];
+    uint64_t  launches;
+    double    total_ms;
+    double    bytes;
+} dgpu_kernel_timing;
+int dgpu_plan_set_timing(dgpu_plan* plan, int enable);
+int dgpu_plan_get_timing(dgpu_plan* plan, dgpu_kernel_timing* out, int max,
+                         int* count, int reset);
+
+/* Plan tables (src/dynasor_preprocess.cpp:291-463): shard ranges of mode n
+ * (K entries each), and the LPT schedule as per-worker counts plus the
+ * concatenated shard lists.  *n_listed receives the number of shards. */
+int dgpu_plan_shards(const dgpu_plan* plan, int n, uint64_t* begin, uint64_t* end);
+int dgpu_plan_schedule(const dgpu_plan* plan, int n, uint32_t* counts,
+                       uint32_t* flat, uint32_t* n_listed);
+
+/* ---- factors ---------------------------------------------------------- */
+/* Y[n] <- host I_n x Rp row-major FP32 (replaces FactorMatrices::Y,
+ * include/dynasor_common.h:604-615). */
+int dgpu_upload_factor(dgpu_plan* plan, int n, const float* Y);
+int dgpu_download_factor(dgpu_plan* plan, int n, float* Y);
+int dgpu_download_yhat(dgpu_plan* plan, int n, float* Yhat);
+int dgpu_download_lambda(dgpu_plan* plan, float* lambda);
+/* Device pointers of Y[n] / Yhat[n] (I_n x Rp FP32), for zero-copy use. */
+int dgpu_factor_device_ptr(dgpu_plan* plan, int n, void** Y, void** Yhat);
+
+/* ---- MTTKRP (replaces SpmttkrpSweep::process, src/dynasor.cpp:352-539,
+ *      and dynasor_process_shard, src/dynasor_kernel.cpp:289-338) ------- */
+/* Mode n MTTKRP into Yhat[n]; under PingPong also remaps the slab for mode
+ * (n+1) % N on the device.  Modes must be called in order 0,1,..,N-1,0,..
+ * (DGPU_ERR_ORDER otherwise).  Asynchronous on the plan stream. */
+int dgpu_mttkrp_mode(dgpu_plan* plan, int n);
+/* All N modes in order (spmttkrp_dynasor, src/dynasor.cpp:545-559). */
+int dgpu_mttkrp_sweep(dgpu_plan* plan);
+/* All-modes single pass from one factor snapshot (Jacobi;
+ * spmttkrp_all_modes_dynasor, src/dynasor.cpp:592-817). */
+int dgpu_mttkrp_all_modes(dgpu_plan* plan);
+/* Host-buffer convenience: upload Y[0..N-1], one sweep, download
+ * Yhat[0..N-1]; returns the device seconds of the sweep in *secs. */
+int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y,
+                           float* const* Yhat, double* secs);
+
+/* Current slab as the next mode's kernel will read it (bit-exact layout
+ * checks against the reference's Tensor after process(n)). */
+int dgpu_download_slab(dgpu_plan* plan, float* vals, uint32_t* const* idx);
+/* NCopy copy k (layout NCopy only). */
+int dgpu_download_copy(dgpu_plan* plan, int k, float* vals, uint32_t* const* idx);
+
+/* ---- CP-ALS (replaces cpals, src/dynasor_cpals.cpp:120-396) ---------- */
+void dgpu_cp_options_default(dgpu_cp_options* opt);
+/* fit_history receives one FP64 fit per iteration (max_iters entries). */
+int  dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt,
+                dgpu_cp_result* res, double* fit_history);
+
+/* ---- small dense kernels (replace la::*, include/dynasor_linalg.h:33-127),
+ *      device pointers, FP32 row-major with leading dimension Rp --------- */
+int dgpu_la_gram(void* stream, const float* Y, uint64_t rows, int R, int Rp, float* G);
+int dgpu_tensor_norm_sq(dgpu_plan* plan, double* norm_sq);
+
+/* ---- CP-OPT forward / adjoint (no reference counterpart: the gradient
+ *      of 0.5*||X - M||^2 over the nonzeros, built from MTTKRP) -------- */
+/* model[i] = sum_r prod_n Y[n][idx_n(i), r] at every nonzero, in the
+ * current slab order (FP32 out). */
+int dgpu_model_values(dgpu_plan* plan, float* model_host);
+/* grad[n] = -(MTTKRP_n(X) - Y[n] * Hadamard_{m!=n}(Y[m]^T Y[m])), the
+ * gradient of 0.5*||X - M||_F^2 w.r.t. Y[n] for the dense CP model M,
+ * written to host I_n x Rp FP32 buffers. */
+int dgpu_cpopt_gradient(dgpu_plan* plan, float* const* grad_host);
+
+/* ---- host loaders (replace load_coo_tensor / save_dnb_tensor /
+ *      dump_factor_matrix_bin, src/dynasor_io.cpp:576-1348) ---------------- */
+/* A host COO tensor owned by the library (free with dgpu_coo_free). */
+typedef struct {
+    int       num_modes;
+    uint64_t  nnz;
+    uint32_t  mode_size[DGPU_MAX_MODES];
+    float*    vals;
+    uint32_t* idx[DGPU_MAX_MODES];
+} dgpu_coo;
+
+/* <path>.dnb when fresh, else parse <path> (.tns) and, when use_cache,
+ * write <path>.dnb (src/dynasor_io.cpp:1184-1261). */
+int  dgpu_load_coo_tensor(const char* path, int use_cache, dgpu_coo* out);
+int  dgpu_load_tns(const char* path, dgpu_coo* out);        /* :576-745  */
+int  dgpu_load_dnb(const char* path, dgpu_coo* out);        /* :805-850  */
+int  dgpu_save_dnb(const char* path, const dgpu_coo* t);    /* :854-893  */
+void dgpu_coo_free(dgpu_coo* t);
+/* DYFM dump of an I x rank_padded factor, padding stripped (:1287-1348). */
+int  dgpu_dump_factor_bin(const char* path, const float* data, uint32_t rows,
+                          int rank, int rank_padded);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DYNASOR_B200_H */
