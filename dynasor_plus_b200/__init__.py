@@ -33,6 +33,7 @@ PINGPONG = 0
 NCOPY = 1
 LAYOUTS = {"pingpong": PINGPONG, "ncopy": NCOPY}
 PRECISIONS = {"fp32": 0, "bf16": 1}
+ACCUMS = {"auto": 0, "rowrun": 1, "private": 2}
 
 
 def padded_rank(R: int) -> int:
@@ -67,7 +68,7 @@ class Plan:
 
     def __init__(self, dims, vals, idx, threads: int, rank: int, layout: str = "pingpong",
                  fiber: bool = True, precision: str = "fp32", device: int = 0,
-                 mn_target=None, stream=None):
+                 mn_target=None, stream=None, accum: str = "auto"):
         L = lib()
         self.N = len(dims)
         self.dims = np.ascontiguousarray(dims, np.uint32)
@@ -89,6 +90,7 @@ class Plan:
         opts.fiber = 1 if fiber else 0
         opts.precision = PRECISIONS[precision]
         opts.device = int(device)
+        opts.accum = ACCUMS[accum]
         self._mn = None
         if mn_target is not None:
             self._mn = np.ascontiguousarray(mn_target, np.uint32)

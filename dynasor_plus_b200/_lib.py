@@ -33,7 +33,8 @@ class TensorDesc(C.Structure):
 
 class PlanOpts(C.Structure):
     _fields_ = [("threads", C.c_int), ("rank", C.c_int), ("layout", C.c_int), ("fiber", C.c_int),
-                ("precision", C.c_int), ("device", C.c_int), ("mn_target", C.POINTER(C.c_uint32))]
+                ("precision", C.c_int), ("device", C.c_int), ("accum", C.c_int),
+                ("mn_target", C.POINTER(C.c_uint32))]
 
 
 class PlanInfo(C.Structure):

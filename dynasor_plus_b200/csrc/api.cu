@@ -104,6 +104,9 @@ int dgpu_plan_create(const dgpu_tensor_desc* t, const dgpu_plan_opts* o, dgpu_pl
     if (o->precision != DGPU_PREC_FP32 && o->precision != DGPU_PREC_BF16) {
         set_error("dgpu_plan_create: unknown precision %d", o->precision); return DGPU_ERR_ARG;
     }
+    if (o->accum < DGPU_ACCUM_AUTO || o->accum > DGPU_ACCUM_PRIVATE) {
+        set_error("dgpu_plan_create: unknown accumulation mode %d", o->accum); return DGPU_ERR_ARG;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

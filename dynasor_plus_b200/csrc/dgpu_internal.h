@@ -118,6 +118,7 @@ struct Plan {
     int       layout = DGPU_LAYOUT_PINGPONG;
     int       fiber = 1;
     int       precision = DGPU_PREC_FP32;
+    int       accum = DGPU_ACCUM_AUTO;
     int       device = 0;
     uint32_t  dims[kMaxModes] = {};
     uint32_t  mn[kMaxModes] = {};

@@ -30,7 +30,7 @@ struct FacPtrs32 {
 
 template <int N, int G, int V>
 __global__ void __launch_bounds__(kThreads)
-k_mttkrp_all(SlabPtrs in, uint64_t nnz, FacPtrs32 F, float* Yh0, float* Yh1, float* Yh2, float* Yh3, float* Yh4, float* Yh5, float* Yh6,
+k_mttkrp_all(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_constant__ FacPtrs32 F, float* Yh0, float* Yh1, float* Yh2, float* Yh3, float* Yh4, float* Yh5, float* Yh6,
              float* Yh7, int Rp)
 {
     float* Yh[8] = {Yh0, Yh1, Yh2, Yh3, Yh4, Yh5, Yh6, Yh7};
@@ -75,7 +75,7 @@ k_mttkrp_all(SlabPtrs in, uint64_t nnz, FacPtrs32 F, float* Yh0, float* Yh1, flo
 // model[i] = sum_r prod_w Y[w][i_w, r]  (one lane group per nonzero)
 template <int N, int G, int V>
 __global__ void __launch_bounds__(kThreads)
-k_model_values(SlabPtrs in, uint64_t nnz, FacPtrs32 F, int Rp, float* __restrict__ out)
+k_model_values(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_constant__ FacPtrs32 F, int Rp, float* __restrict__ out)
 {
     const int gl = threadIdx.x % G;
     const int C4 = Rp >> 2;

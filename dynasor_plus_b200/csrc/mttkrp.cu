@@ -1,24 +1,35 @@
 // ============================================================================
 //  mttkrp.cu -- mode-n sparse MTTKRP over a FLYCOO slab (sm_100a).
 //
-//  Replaces the reference's per-nnz kernel (src/dynasor_kernel.cpp:91-229,
+//  Replaces the reference's per-nnz kernels (src/dynasor_kernel.cpp:91-229,
 //  fiber variant :365-489).  Arithmetic per nonzero is the reference's:
 //      prod = val * Y[w0][i_w0, :]            (w0 = n==0 ? 1 : 0)
 //      prod *= Y[w][i_w, :]                   (every other w except w_last)
-//      Yhat[n][i_n, :] = fma(prod, Y[w_last][i_wl, :], Yhat[n][i_n, :])
-//  (for N == 2 the last step is an add).  Gathers and products are FP32 (or
-//  BF16 gathers widened to FP32); accumulation is FP32.
+//      Yhat[n][i_n, :] += prod * Y[w_last][i_wl, :]
+//  (for N == 2 the last factor is absent).  Gathers are FP32 or BF16 widened
+//  to FP32; accumulation is FP32.  This is a gather, not a contraction: no
+//  tensor cores.
 //
-//  GPU mapping.  One CTA per work tile (<= kTile consecutive slab positions
-//  of one super-shard, tiles in the reference's processing order).  A
-//  "lane group" of G lanes owns one nonzero at a time; lane g holds float4
-//  column chunk g (+ v*G) of the rank, so one warp-wide LDG.128 gathers
-//  32/G factor rows.  Each group walks a contiguous run of the tile and
-//  keeps the current output row's partial sum in registers; the sum is
-//  written with one vector atomic (red.global.add.v4.f32) when the row
-//  changes.  On a fiber-sorted slab (rows contiguous, the reference's
-//  DenseFiber layout) that is one atomic per row segment; on an unsorted
-//  slab it degrades to one per nonzero, which stays correct.
+//  Two accumulation schemes (dgpu_plan_opts.accum):
+//
+//  PRIVATE  (k_mttkrp_priv) -- the Yhat block of the current super-shard
+//      (m_n rows x Rp) is held in shared memory.  Each nonzero adds its row
+//      contribution with shared-memory atomics (lane c owns columns c,
+//      c+32, ..., so the 32 lanes of a warp hit 32 distinct banks).  Slab
+//      order inside a shard is irrelevant.  A persistent CTA walks a
+//      contiguous run of tiles in processing order and flushes the block to
+//      global Yhat (vector atomics, touched rows only) when the shard
+//      changes and at the end, so global atomics scale with rows, not with
+//      nonzeros.
+//
+//  ROWRUN   (k_mttkrp_rowrun) -- a lane group (G lanes, float4 columns)
+//      walks a contiguous run of a tile and keeps the current row's partial
+//      sum in registers, flushing with one vector atomic per row segment.
+//      Ideal on fiber-sorted slabs (rows contiguous); any order is correct.
+//
+//  Both read the slab exactly once.  Metadata of 32 consecutive nonzeros
+//  is fetched by the 32 lanes of a warp with coalesced loads; factor rows
+//  are gathered with one warp-coalesced load per row.
 // ============================================================================
 #include "dgpu_internal.h"
 
@@ -28,25 +39,10 @@ namespace dgpu {
 
 namespace {
 
-constexpr int kThreads = 256;
-
 struct FacPtrs {
     const float*         Y[kMaxModes];
     const __nv_bfloat16* Yb[kMaxModes];
 };
-
-template <bool BF>
-__device__ __forceinline__ float4 gather4(const FacPtrs& F, int w, uint32_t row, int Rp, int c4) {
-    if constexpr (BF) {
-        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(F.Yb[w] + (size_t)row * Rp) + c4);
-        const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162*>(&raw.x);
-        const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162*>(&raw.y);
-        const float2 a = __bfloat1622float2(lo), b = __bfloat1622float2(hi);
-        return make_float4(a.x, a.y, b.x, b.y);
-    } else {
-        return __ldg(reinterpret_cast<const float4*>(F.Y[w] + (size_t)row * Rp) + c4);
-    }
-}
 
 __device__ __forceinline__ float4 mul4(float4 a, float4 b) {
     return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
@@ -62,23 +58,55 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
     return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
 
-// Elements per batch: keeps (N-1)*V*U float4 gathers in flight per lane.
+template <bool BF>
+__device__ __forceinline__ float4 gather4(const FacPtrs& F, int w, uint32_t row, int Rp, int c4) {
+    if constexpr (BF) {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2*>(F.Yb[w] + (size_t)row * Rp) + c4);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    } else {
+        return __ldg(reinterpret_cast<const float4*>(F.Y[w] + (size_t)row * Rp) + c4);
+    }
+}
+
+// Compile-time loop: f(integral_constant<int, 0..K-1>) so register arrays
+// indexed by the loop variable stay in registers.
+template <int I, int K, typename Fn>
+__device__ __forceinline__ void static_for(Fn&& f) {
+    if constexpr (I < K) {
+        f(std::integral_constant<int, I>{});
+        static_for<I + 1, K>(f);
+    }
+}
+
+template <bool BF>
+__device__ __forceinline__ float gather1(const FacPtrs& F, int w, uint32_t row, int RP, int c) {
+    if constexpr (BF) return __bfloat162float(F.Yb[w][(size_t)row * RP + c]);
+    else return __ldg(F.Y[w] + (size_t)row * RP + c);
+}
+
+// ===========================================================================
+//  ROWRUN
+// ===========================================================================
+constexpr int kRunThreads = 256;
+
 template <int N, int V>
-struct Batch {
+struct RunBatch {
     static constexpr int kWork = (N - 1) * V;
     static constexpr int U = kWork <= 2 ? 4 : (kWork <= 4 ? 2 : 1);
 };
 
 template <int N, int G, int V, bool BF>
-__global__ void __launch_bounds__(kThreads)
-k_mttkrp_rowrun(SlabPtrs in, const uint32_t* __restrict__ rowcol,
-                const Tile* __restrict__ tiles, FacPtrs F, float* __restrict__ Yhat,
-                int n, int w0, int wl, int Rp)
+__global__ void __launch_bounds__(kRunThreads)
+k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const uint32_t* __restrict__ rowcol,
+                const Tile* __restrict__ tiles, const __grid_constant__ FacPtrs F,
+                float* __restrict__ Yhat, int n, int w0, int wl, int Rp)
 {
-    constexpr int U = Batch<N, V>::U;
+    constexpr int U = RunBatch<N, V>::U;
+    constexpr int kGroups = kRunThreads / G;
     const int gl = threadIdx.x % G;
     const int grp = threadIdx.x / G;
-    constexpr int kGroups = kThreads / G;
     const int C4 = Rp >> 2;
 
     const Tile tl = tiles[blockIdx.x];
@@ -91,53 +119,44 @@ k_mttkrp_rowrun(SlabPtrs in, const uint32_t* __restrict__ rowcol,
     for (int v = 0; v < V; ++v) acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
     uint32_t cur = 0xffffffffu;
 
-    auto flush = [&](uint32_t row) {
-        float4* out = reinterpret_cast<float4*>(Yhat + (size_t)row * Rp);
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const int c4 = gl + v * G;
-            if (V == 1 || c4 < C4) atomicAdd(out + c4, acc[v]);
-            acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    };
-
     for (uint32_t j0 = gb; j0 < ge; j0 += U) {
         float    val[U];
         uint32_t row[U];
-        uint32_t id[U][N];
-        bool     ok[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            ok[u] = (j0 + u) < ge;
-            const uint32_t p = tl.begin + (ok[u] ? j0 + u : gb);
-            val[u] = __ldg(in.vals + p);
-            row[u] = __ldg(rowcol + p);
-#pragma unroll
-            for (int w = 0; w < N; ++w) id[u][w] = (w == n) ? 0u : __ldg(in.idx[w] + p);
-        }
-        float4 y[U][N][V];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
+        float4   y[U][N][V];
+        static_for<0, U>([&](auto uc) {
+            constexpr int u = decltype(uc)::value;
+            const bool ok = (j0 + u) < ge;
+            const uint32_t p = tl.begin + (ok ? j0 + u : gb);
+            val[u] = ok ? __ldg(in.vals + p) : 0.f;
+            row[u] = ok ? __ldg(rowcol + p) : cur;
 #pragma unroll
             for (int w = 0; w < N; ++w) {
-                if (w == n) continue;
+                const uint32_t id = (w == n) ? 0u : __ldg(in.idx[w] + p);
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     const int c4 = gl + v * G;
-                    y[u][w][v] = (V == 1 || c4 < C4) ? gather4<BF>(F, w, id[u][w], Rp, c4)
-                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+                    y[u][w][v] = (w != n && (V == 1 || c4 < C4)) ? gather4<BF>(F, w, id, Rp, c4)
+                                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
             }
+        });
+        static_for<0, U>([&](auto uc) {
+            constexpr int u = decltype(uc)::value;
+            const bool flush = (j0 + u < ge) && row[u] != cur && cur != 0xffffffffu;
+            if (flush) {
+                float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (!ok[u]) continue;
-            if (row[u] != cur) {
-                if (cur != 0xffffffffu) flush(cur);
-                cur = row[u];
+                for (int v = 0; v < V; ++v) {
+                    const int c4 = gl + v * G;
+                    if (V == 1 || c4 < C4) atomicAdd(out + c4, acc[v]);
+                    acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
             }
-            // Non-target modes in increasing order: the first starts the
+            if (j0 + u < ge) cur = row[u];
+            if (j0 + u >= ge) val[u] = 0.f;
+            // non-target modes in increasing order: the first starts the
             // product (w0), the middle ones multiply, the last (w_last) is
-            // fused into the accumulate -- the reference's operation order.
+            // fused into the accumulate -- the reference's order
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 float4 pr = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -150,49 +169,244 @@ k_mttkrp_rowrun(SlabPtrs in, const uint32_t* __restrict__ rowcol,
                 }
                 if (wl < 0) acc[v] = add4(acc[v], pr);
             }
+        });
+    }
+    if (cur != 0xffffffffu) {
+        float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int c4 = gl + v * G;
+            if (V == 1 || c4 < C4) atomicAdd(out + c4, acc[v]);
         }
     }
-    if (cur != 0xffffffffu) flush(cur);
 }
 
-template <int N, bool BF>
-int dispatch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
-                    const FacPtrs& F, int w0, int wl)
+// ===========================================================================
+//  PRIVATE
+// ===========================================================================
+constexpr int kPrivThreads = 1024;
+constexpr int kPrivWarps = kPrivThreads / 32;
+
+template <int N>
+struct Slot {
+    static constexpr int kWords = (1 + N + 3) / 4 * 4;   // 16-byte multiple
+};
+
+template <int N, int C>
+struct PrivBatch {
+    static constexpr int kWork = (N - 1) * C;
+    static constexpr int U = kWork <= 2 ? 8 : (kWork <= 4 ? 4 : (kWork <= 8 ? 2 : 1));
+};
+
+__host__ __device__ constexpr uint32_t priv_flag_words(uint32_t m) {
+    return ((m + 31) / 32 + 3) / 4 * 4;
+}
+
+template <int N, int RP, bool BF>
+__global__ void __launch_bounds__(kPrivThreads, 1)
+k_mttkrp_priv(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ tiles,
+              uint32_t ntiles, uint32_t per_cta, const __grid_constant__ FacPtrs F,
+              float* __restrict__ Yhat, int n, int w0, int wl, int shift_n, uint32_t dim_n)
 {
-    const int C4 = p.Rp / 4;
-    const SlabPtrs sp = slab_in(in, p.N);
-    float* out = p.Yhat[n];
-#define DGPU_LAUNCH(G, V) \
-    k_mttkrp_rowrun<N, G, V, BF><<<ntiles, kThreads, 0, p.stream>>>(sp, in.idx[n], tiles, F, out, n, w0, wl, p.Rp)
-    if (C4 == 4) DGPU_LAUNCH(4, 1);
-    else if (C4 == 8) DGPU_LAUNCH(8, 1);
-    else if (C4 == 16) DGPU_LAUNCH(16, 1);
-    else if (C4 == 32) DGPU_LAUNCH(32, 1);
-    else if (C4 <= 64) DGPU_LAUNCH(32, 2);
-    else if (C4 <= 96) DGPU_LAUNCH(32, 3);
-    else if (C4 <= 128) DGPU_LAUNCH(32, 4);
-    else if (C4 <= 256) DGPU_LAUNCH(32, 8);
-    else {
-        set_error("mttkrp: rank_padded %d exceeds the supported maximum 1024", p.Rp);
-        return DGPU_ERR_ARG;
+    constexpr int G = RP < 32 ? RP : 32;          // lanes per nonzero
+    constexpr int E = 32 / G;                     // nonzeros per warp step
+    constexpr int C = RP / G;                     // columns per lane (stride G)
+    constexpr int SW = Slot<N>::kWords;
+    constexpr int U = PrivBatch<N, C>::U;
+
+    extern __shared__ float sm[];
+    const uint32_t m = 1u << shift_n;
+    float* yb = sm;                                                        // m x RP
+    uint32_t* touched = reinterpret_cast<uint32_t*>(yb + (size_t)m * RP);  // bit per row
+    uint32_t* slots = touched + priv_flag_words(m);                        // warps x 32 x SW
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* ws = slots + (size_t)warp * 32 * SW;
+
+    for (uint32_t i = threadIdx.x; i < m * RP; i += blockDim.x) yb[i] = 0.f;
+    for (uint32_t i = threadIdx.x; i < priv_flag_words(m); i += blockDim.x) touched[i] = 0u;
+    __syncthreads();
+
+    const uint32_t t0 = blockIdx.x * per_cta;
+    const uint32_t t1 = min(ntiles, t0 + per_cta);
+    uint32_t cur_shard = 0xffffffffu;
+    const int sub = lane / G;                 // which nonzero of a step this lane serves
+    const int gl = lane % G;                  // lane within its group
+
+    for (uint32_t t = t0; t <= t1; ++t) {
+        const bool last = (t == t1);
+        const uint32_t shard = last ? 0xfffffffeu : tiles[t].shard;
+        if (shard != cur_shard && cur_shard != 0xffffffffu) {
+            // flush the finished shard block: one warp per touched row
+            __syncthreads();
+            const uint32_t base = cur_shard << shift_n;
+            for (uint32_t r = warp; r < m; r += kPrivWarps) {
+                if (!(touched[r >> 5] & (1u << (r & 31)))) continue;
+                const uint32_t grow = base + r;
+                if (grow < dim_n)
+                    for (int c = lane; c < RP; c += 32) {
+                        atomicAdd(Yhat + (size_t)grow * RP + c, yb[(size_t)r * RP + c]);
+                        yb[(size_t)r * RP + c] = 0.f;
+                    }
+            }
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < priv_flag_words(m); i += blockDim.x) touched[i] = 0u;
+            __syncthreads();
+        }
+        if (last) break;
+        cur_shard = shard;
+        const Tile tl = tiles[t];
+        const uint32_t rbase = tl.shard << shift_n;
+        const uint32_t nbat = (tl.count + 31) / 32;
+        for (uint32_t b = warp; b < nbat; b += kPrivWarps) {
+            const uint32_t j = b * 32 + lane;
+            if (j < tl.count) {
+                const uint32_t pidx = tl.begin + j;
+                ws[lane * SW] = __float_as_uint(__ldg(in.vals + pidx));
+#pragma unroll
+                for (int w = 0; w < N; ++w) ws[lane * SW + 1 + w] = __ldg(in.idx[w] + pidx);
+            }
+            __syncwarp();
+            const int cnt = (int)min(32u, tl.count - b * 32);
+            for (int e0 = 0; e0 < cnt; e0 += U * E) {
+                float val[U];
+                uint32_t rowl[U];
+                float y[U][N][C];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = e0 + u * E + sub;
+                    const bool ok = e < cnt;
+                    const uint32_t* sl = ws + (ok ? e : 0) * SW;
+                    val[u] = ok ? __uint_as_float(sl[0]) : 0.f;
+                    rowl[u] = ok ? sl[1 + n] - rbase : 0xffffffffu;
+#pragma unroll
+                    for (int w = 0; w < N; ++w) {
+                        if (w == n) continue;
+                        const uint32_t id = sl[1 + w];
+#pragma unroll
+                        for (int c = 0; c < C; ++c) y[u][w][c] = gather1<BF>(F, w, id, RP, gl + c * G);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (rowl[u] == 0xffffffffu) continue;
+                    float* dst = yb + (size_t)rowl[u] * RP + gl;
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        float pr = val[u];
+#pragma unroll
+                        for (int w = 0; w < N; ++w)
+                            if (w != n) pr *= y[u][w][c];
+                        atomicAdd(dst + c * G, pr);
+                    }
+                    if (gl == 0) atomicOr(touched + (rowl[u] >> 5), 1u << (rowl[u] & 31));
+                }
+            }
+            __syncwarp();
+        }
     }
-#undef DGPU_LAUNCH
+}
+
+size_t priv_smem_bytes(int N, uint32_t m, int RP) {
+    const int sw = (1 + N + 3) / 4 * 4;
+    return (size_t)m * RP * 4 + (size_t)priv_flag_words(m) * 4 + (size_t)kPrivWarps * 32 * sw * 4;
+}
+
+constexpr size_t kPrivMaxSmem = 200 * 1024;
+
+template <int N, bool BF>
+int launch_priv(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
+                const FacPtrs& F, int w0, int wl)
+{
+    const uint32_t m = 1u << p.shift[n];
+    const size_t smem = priv_smem_bytes(N, m, p.Rp);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
+    const int per_sm = smem <= 100 * 1024 ? 2 : 1;
+    const uint32_t want = std::max<uint32_t>(1, std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm)));
+    const uint32_t per_cta = (ntiles + want - 1) / want;
+    const uint32_t grid = (ntiles + per_cta - 1) / per_cta;
+    const SlabPtrs sp = slab_in(in, p.N);
+#define DGPU_PRIV(RPV)                                                                           \
+    do {                                                                                         \
+        auto k = k_mttkrp_priv<N, RPV, BF>;                                                      \
+        DGPU_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        k<<<grid, kPrivThreads, smem, p.stream>>>(sp, tiles, ntiles, per_cta, F, p.Yhat[n], n,    \
+                                                  w0, wl, p.shift[n], p.dims[n]);               \
+    } while (0)
+    switch (p.Rp) {
+        case 16: DGPU_PRIV(16); break;
+        case 32: DGPU_PRIV(32); break;
+        case 64: DGPU_PRIV(64); break;
+        default: DGPU_PRIV(128); break;
+    }
+#undef DGPU_PRIV
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
 }
 
+template <int N, bool BF>
+int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
+                  const FacPtrs& F, int w0, int wl)
+{
+    const int C4 = p.Rp / 4;
+    const SlabPtrs sp = slab_in(in, p.N);
+    float* out = p.Yhat[n];
+#define DGPU_RUN(G, V)                                                                        \
+    k_mttkrp_rowrun<N, G, V, BF><<<ntiles, kRunThreads, 0, p.stream>>>(sp, in.idx[n], tiles, F, \
+                                                                       out, n, w0, wl, p.Rp)
+    if (C4 == 4) DGPU_RUN(4, 1);
+    else if (C4 == 8) DGPU_RUN(8, 1);
+    else if (C4 == 16) DGPU_RUN(16, 1);
+    else if (C4 == 32) DGPU_RUN(32, 1);
+    else if (C4 <= 64) DGPU_RUN(32, 2);
+    else if (C4 <= 96) DGPU_RUN(32, 3);
+    else if (C4 <= 128) DGPU_RUN(32, 4);
+    else if (C4 <= 256) DGPU_RUN(32, 8);
+    else {
+        set_error("mttkrp: rank_padded %d exceeds the supported maximum 1024", p.Rp);
+        return DGPU_ERR_ARG;
+    }
+#undef DGPU_RUN
+    DGPU_CUDA(cudaGetLastError());
+    return DGPU_OK;
+}
+
+}  // namespace
+
+// Which accumulation scheme mode n uses under this plan.
+int mttkrp_scheme(const Plan& p, int n) {
+    const bool priv_ok = (p.Rp == 16 || p.Rp == 32 || p.Rp == 64 || p.Rp == 128) &&
+                         priv_smem_bytes(p.N, 1u << p.shift[n], p.Rp) <= kPrivMaxSmem;
+    if (p.accum == DGPU_ACCUM_ROWRUN) return DGPU_ACCUM_ROWRUN;
+    if (p.accum == DGPU_ACCUM_PRIVATE) return priv_ok ? DGPU_ACCUM_PRIVATE : DGPU_ACCUM_ROWRUN;
+    const bool sorted = p.fiber && p.kclass[n] == 2;
+    if (!sorted && priv_ok) return DGPU_ACCUM_PRIVATE;
+    return DGPU_ACCUM_ROWRUN;
+}
+
+namespace {
+
+template <int N, bool BF>
+int launch_n(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
+             const FacPtrs& F, int w0, int wl)
+{
+    if (mttkrp_scheme(p, n) == DGPU_ACCUM_PRIVATE)
+        return launch_priv<N, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+    return launch_rowrun<N, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+}
+
 template <bool BF>
-int dispatch_modes(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
-                   const FacPtrs& F, int w0, int wl)
+int launch_modes(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
+                 const FacPtrs& F, int w0, int wl)
 {
     switch (p.N) {
-        case 2: return dispatch_rowrun<2, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-        case 3: return dispatch_rowrun<3, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-        case 4: return dispatch_rowrun<4, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-        case 5: return dispatch_rowrun<5, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-        case 6: return dispatch_rowrun<6, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-        case 7: return dispatch_rowrun<7, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-        case 8: return dispatch_rowrun<8, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 2: return launch_n<2, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 3: return launch_n<3, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 4: return launch_n<4, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 5: return launch_n<5, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 6: return launch_n<6, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 7: return launch_n<7, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+        case 8: return launch_n<8, BF>(p, n, in, tiles, ntiles, F, w0, wl);
         default:
             set_error("mttkrp: %d modes unsupported (2..8)", p.N);
             return DGPU_ERR_ARG;
@@ -233,8 +447,8 @@ int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
     for (int w = 0; w < p.N; ++w)
         if (w != n) bytes += (double)p.dims[w] * p.R * (bf ? 2.0 : 4.0);
     LaunchTimer t(p, KK_MTTKRP, bytes);
-    if (bf) return dispatch_modes<true>(p, n, in, tiles, ntiles, F, w0, wl);
-    return dispatch_modes<false>(p, n, in, tiles, ntiles, F, w0, wl);
+    if (bf) return launch_modes<true>(p, n, in, tiles, ntiles, F, w0, wl);
+    return launch_modes<false>(p, n, in, tiles, ntiles, F, w0, wl);
 }
 
 }  // namespace dgpu

@@ -159,7 +159,7 @@ k_scan_down(const uint32_t* __restrict__ in, size_t n, const uint32_t* __restric
 // One CTA per tile.  Warp w owns the w-th contiguous eighth of the tile, so
 // tile order = warp order = lane order within a 32-element step.
 __global__ void __launch_bounds__(kPartThreads)
-k_part_scatter(SlabPtrs in, SlabOut out, int N, const Tile* __restrict__ tiles,
+k_part_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out, int N, const Tile* __restrict__ tiles,
                uint32_t ntiles, const uint32_t* __restrict__ off, int key_mode,
                int shift, uint32_t mask, uint32_t nb)
 {

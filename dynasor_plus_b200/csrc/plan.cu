@@ -198,7 +198,7 @@ struct Geom {
     uint32_t binoff[kMaxModes];
 };
 
-__global__ void k_shard_counts(SlabPtrs in, int N, uint64_t nnz, Geom g, uint32_t total,
+__global__ void k_shard_counts(const __grid_constant__ SlabPtrs in, int N, uint64_t nnz, Geom g, uint32_t total,
                                int use_smem, unsigned long long* __restrict__ counts,
                                int* __restrict__ err)
 {
@@ -290,6 +290,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     p.layout = o.layout;
     p.fiber = o.fiber ? 1 : 0;
     p.precision = o.precision;
+    p.accum = o.accum;
     p.device = o.device;
     DGPU_CUDA(cudaSetDevice(p.device));
     if (!p.stream) {

@@ -56,6 +56,16 @@ extern "C" {
 #define DGPU_PREC_FP32       0   /* FP32 gathers, FP32 accumulation       */
 #define DGPU_PREC_BF16       1   /* BF16 gathers (FP32 master factors)    */
 
+/* How the MTTKRP kernel accumulates Yhat rows. */
+#define DGPU_ACCUM_AUTO      0   /* ROWRUN on fiber-sorted modes, else
+                                    PRIVATE when the shard block fits     */
+#define DGPU_ACCUM_ROWRUN    1   /* registers per row run + vector atomics
+                                    at run ends (fast when rows are
+                                    contiguous, i.e. fiber-sorted)       */
+#define DGPU_ACCUM_PRIVATE   2   /* the super-shard's Yhat block in shared
+                                    memory (any slab order; needs
+                                    m_n * Rp * 4 <= ~200 KB)              */
+
 typedef struct dgpu_plan dgpu_plan;   /* opaque */
 
 /* Host COO tensor description (0-based indices). */
@@ -77,6 +87,7 @@ typedef struct {
                                      DYN_FIBER_OFF=1                     */
     int       precision;          /* DGPU_PREC_*                         */
     int       device;             /* CUDA device ordinal                 */
+    int       accum;              /* DGPU_ACCUM_*                        */
     const uint32_t* mn_target;    /* optional rows-per-shard override
                                      (NULL = pick like pick_mn)          */
 } dgpu_plan_opts;

@@ -95,7 +95,7 @@ def _oracle_lib():
         L.orc_cpals_f64.restype = C.c_int
         L.orc_cpals_f64.argtypes = [C.c_int, C.c_uint64, _u32p, _f32p, C.c_void_p, C.c_int,
                                     C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
-                                    _f64p, _f64p]
+                                    _f64p, _f64p, C.c_int]
         _olib = L
     return _olib
 
@@ -223,9 +223,10 @@ def uniform_factors(seed, dims, R):
     return Y
 
 
-def cpals_f64(dims, vals, idx, R, max_iters, tol, seed=42, ridge=1e-10, Y0=None):
-    """FP64 Gauss-Seidel CP-ALS from the reference's seed-`seed` N(0,1) init
-    (or from Y0).  Returns (fit_history, Y, lambda)."""
+def cpals_f64(dims, vals, idx, R, max_iters, tol, seed=42, ridge=1e-10, Y0=None, jacobi=False):
+    """FP64 CP-ALS (Gauss-Seidel, or Jacobi: all MTTKRPs from the iteration's
+    starting factors) from the reference's seed-`seed` N(0,1) init (or from
+    Y0).  Returns (fit_history, Y, lambda)."""
     L = _oracle_lib()
     N = len(dims)
     Rp = padded_rank(R)
@@ -238,7 +239,7 @@ def cpals_f64(dims, vals, idx, R, max_iters, tol, seed=42, ridge=1e-10, Y0=None)
     idx = [np.ascontiguousarray(i, np.uint32) for i in idx]
     it = L.orc_cpals_f64(N, len(vals), np.ascontiguousarray(dims, np.uint32),
                          np.ascontiguousarray(vals, np.float32), _ptr_array(idx), R, Rp,
-                         max_iters, tol, ridge, _ptr_array(Y), fit, lam)
+                         max_iters, tol, ridge, _ptr_array(Y), fit, lam, 1 if jacobi else 0)
     return fit[:it], Y, lam
 
 

@@ -409,7 +409,7 @@ void orc_uniform_factors(uint64_t seed, int N, const uint32_t* dims, int R,
 int orc_cpals_f64(int N, uint64_t nnz, const uint32_t* dims, const float* vals,
                   const uint32_t* const* idx, int R, int Rp, int max_iters,
                   double tol, double ridge, float* const* Yio,
-                  double* fit_hist, double* lambda_out)
+                  double* fit_hist, double* lambda_out, int jacobi)
 {
     std::vector<std::vector<double>> Y(N), Yh(N), G(N);
     for (int n = 0; n < N; ++n) {
@@ -433,19 +433,27 @@ int orc_cpals_f64(int N, uint64_t nnz, const uint32_t* dims, const float* vals,
     std::vector<double> lam(R, 1.0), V((size_t)R * R), t(R);
     double fit_prev = 0;
     int it = 0;
-    for (; it < max_iters; ++it) {
-        for (int n = 0; n < N; ++n) {
-            std::fill(Yh[n].begin(), Yh[n].end(), 0.0);
-            for (uint64_t i = 0; i < nnz; ++i) {
-                for (int r = 0; r < R; ++r) t[r] = vals[i];
-                for (int w = 0; w < N; ++w) {
-                    if (w == n) continue;
-                    const double* y = &Y[w][(size_t)idx[w][i] * R];
-                    for (int r = 0; r < R; ++r) t[r] *= y[r];
-                }
-                double* o = &Yh[n][(size_t)idx[n][i] * R];
-                for (int r = 0; r < R; ++r) o[r] += t[r];
+    auto mttkrp = [&](int n) {
+        std::fill(Yh[n].begin(), Yh[n].end(), 0.0);
+        for (uint64_t i = 0; i < nnz; ++i) {
+            for (int r = 0; r < R; ++r) t[r] = vals[i];
+            for (int w = 0; w < N; ++w) {
+                if (w == n) continue;
+                const double* y = &Y[w][(size_t)idx[w][i] * R];
+                for (int r = 0; r < R; ++r) t[r] *= y[r];
             }
+            double* o = &Yh[n][(size_t)idx[n][i] * R];
+            for (int r = 0; r < R; ++r) o[r] += t[r];
+        }
+    };
+    for (; it < max_iters; ++it) {
+        // Jacobi: every MTTKRP from the factors at the start of the
+        // iteration (src/dynasor_cpals.cpp:270-278); the per-mode solves
+        // below still use the freshest Grams.
+        if (jacobi)
+            for (int n = 0; n < N; ++n) mttkrp(n);
+        for (int n = 0; n < N; ++n) {
+            if (!jacobi) mttkrp(n);
             for (int a = 0; a < R * R; ++a) V[a] = 1.0;
             for (int m = 0; m < N; ++m)
                 if (m != n) for (int a = 0; a < R * R; ++a) V[a] *= G[m][a];

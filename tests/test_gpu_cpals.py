@@ -58,23 +58,18 @@ def test_convergence_stop_rule():
     assert all(abs(h[i] - h[i - 1]) >= 1e-4 for i in range(1, len(h) - 1))
 
 
-def test_jacobi_runs_and_improves(bindings):
-    """All-modes (Jacobi) updates from one snapshot; its printed fit uses a
-    stale Yhat like the reference's, so check the true FP64 fit instead."""
+def test_jacobi_matches_fp64_jacobi_oracle(bindings):
+    """All-modes (Jacobi): every MTTKRP from the iteration's starting factors
+    (src/dynasor_cpals.cpp:270-278).  Jacobi ALS need not converge, and its
+    printed fit uses the stale Yhat exactly like the reference's, so the
+    check is trajectory parity with the FP64 Jacobi oracle."""
     g, dims, idx, p = _golden_plan()
     R = int(g["R"])
-    r = p.cpals(max_iters=20, tol=0.0, seed=42, kernel="jacobi")
-    assert r["iters_done"] == 20
-    Y = [p.factor(n) for n in range(len(dims))]
-    lam = p.lam()
-    m = bindings.model_values(idx, Y, R, lam)
-    x = g["vals"].astype(np.float64)
-    # ||X - M||^2 over all cells = ||X||^2 - 2<X,M> + ||M||^2
-    G = [Y[n][:, :R].astype(np.float64).T @ Y[n][:, :R] for n in range(len(dims))]
-    H = np.ones((R, R))
-    for Gn in G:
-        H *= Gn
-    l64 = lam.astype(np.float64)
-    res2 = x @ x - 2 * x @ m + l64 @ H @ l64
-    fit = 1 - np.sqrt(max(res2, 0)) / np.sqrt(x @ x)
-    assert fit > 0.9
+    r = p.cpals(max_iters=6, tol=0.0, seed=42, kernel="jacobi")
+    assert r["iters_done"] == 6
+    fit64, Y64, lam64 = bindings.cpals_f64(dims, g["vals"], idx, R, 6, 0.0, seed=42, jacobi=True)
+    # Jacobi sweeps are not contractive, so FP32-vs-FP64 MTTKRP rounding
+    # grows from ~1e-7 to ~1e-4 over 6 iterations
+    assert np.max(np.abs(r["fit_history"] - fit64)) < 1e-3
+    for n in range(len(dims)):
+        assert rel_fro(p.factor(n)[:, :R], Y64[n][:, :R]) < 1e-2
