@@ -58,12 +58,14 @@ const char* last_error();
     } while (0)
 
 // One work tile: `count` consecutive slab positions starting at `begin`,
-// all inside super-shard `shard` of the tile table's mode.
+// all inside super-shard `shard` of the tile table's mode.  For segmented
+// partitions (one independent counting sort per shard) `seg_first` is the
+// index of the first tile of the same shard in the tile array.
 struct Tile {
     uint32_t begin;
     uint32_t count;
     uint32_t shard;
-    uint32_t pad;
+    uint32_t seg_first;
 };
 
 // SoA slab on the device.
@@ -141,6 +143,9 @@ struct Plan {
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for
     Tile*        tiles_d[kMaxModes] = {nullptr};
+    Tile*        ftiles_d[kMaxModes] = {nullptr};  // slab-order tiles per shard (fiber sort)
+    uint32_t*    fseg_d[kMaxModes] = {nullptr};    // tiles per shard, [K_n]
+    uint32_t     nftiles[kMaxModes] = {};
     Tile*        ident_tiles_d = nullptr;       // identity order over [0, nnz)
     uint32_t     n_ident_tiles = 0;
     float*       Y[kMaxModes] = {nullptr};
@@ -191,9 +196,14 @@ int launch_shard_counts(Plan& p, const Slab& s, uint64_t* counts_d, size_t total
 // written to `out` ordered by key = (idx[key_mode] >> key_shift) & key_mask
 // (buckets < nb <= kMaxBuckets), each bucket starting at `base_off` +
 // (elements of all smaller buckets), stably.  Uses p.part_cnt/part_off.
+// With `seg_n` (tiles per shard, indexed by Tile::shard) the partition is
+// segmented: every shard is sorted independently inside its own range.
 int stable_partition(Plan& p, const Slab& in, const Tile* tiles, uint32_t ntiles,
                      int key_mode, int key_shift, uint32_t key_mask, uint32_t nb,
-                     const Slab& out);
+                     const Slab& out, const uint32_t* seg_n = nullptr);
+// Fiber sort of mode n (stable sort of every mode-n shard by row) from
+// slab[src] ping-ponging with slab[other]; *result = slab holding it.
+int fiber_sort(Plan& p, int n, int src, int other, int* result);
 // Stable sort of the sequence listed by `tiles` over slab[a] by the key
 // (idx[key_mode] >> key_shift) < key_limit, any key range: one partition
 // pass per least-significant digit, ping-ponging between slab[a] and

@@ -90,6 +90,7 @@ __device__ __forceinline__ float gather1(const FacPtrs& F, int w, uint32_t row, 
 //  ROWRUN
 // ===========================================================================
 constexpr int kRunThreads = 256;
+constexpr int kRunWarps = kRunThreads / 32;
 
 template <int N, int V>
 struct RunBatch {
@@ -97,86 +98,139 @@ struct RunBatch {
     static constexpr int U = kWork <= 2 ? 4 : (kWork <= 4 ? 2 : 1);
 };
 
+// One CTA per tile.  Warp w owns the w-th contiguous slice of the tile and
+// lane group g (G lanes) the g-th contiguous sub-slice of that, so a group
+// sees every row run of its sub-slice in order.  Per chunk of CH nonzeros
+// the group's lanes load the metadata with coalesced loads into a small
+// shared slot array (prefetching the next chunk into registers), then walk
+// the chunk U nonzeros at a time: U x (N-1) float4 gathers in flight per
+// lane, products in registers, one vector atomic per finished row run.
 template <int N, int G, int V, bool BF>
-__global__ void __launch_bounds__(kRunThreads)
-k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const uint32_t* __restrict__ rowcol,
-                const Tile* __restrict__ tiles, const __grid_constant__ FacPtrs F,
-                float* __restrict__ Yhat, int n, int w0, int wl, int Rp)
+__global__ void __launch_bounds__(kRunThreads, 3)
+k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ tiles,
+                const __grid_constant__ FacPtrs F, float* __restrict__ Yhat,
+                int n, int w0, int wl, int Rp)
 {
     constexpr int U = RunBatch<N, V>::U;
-    constexpr int kGroups = kRunThreads / G;
-    const int gl = threadIdx.x % G;
-    const int grp = threadIdx.x / G;
+    constexpr int NG = 32 / G;                    // groups per warp
+    constexpr int CH = G >= 16 ? G : 16;          // nonzeros staged per group per chunk
+    constexpr int LPE = CH / G;                   // nonzeros loaded per lane per chunk
+    constexpr int SW = (1 + N + 3) / 4 * 4;       // words per slot
+    __shared__ uint32_t slots[kRunWarps][NG][CH][SW];
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / G, gl = lane % G;
     const int C4 = Rp >> 2;
 
     const Tile tl = tiles[blockIdx.x];
-    const uint32_t per = (tl.count + kGroups - 1) / kGroups;
-    const uint32_t gb = min(tl.count, (uint32_t)grp * per);
-    const uint32_t ge = min(tl.count, gb + per);
+    const uint32_t per_w = (tl.count + kRunWarps - 1) / kRunWarps;
+    const uint32_t wb = min(tl.count, (uint32_t)warp * per_w);
+    const uint32_t we = min(tl.count, wb + per_w);
+    const uint32_t per_g = (we - wb + NG - 1) / NG;          // warp-uniform
+    const uint32_t gb = min(we, wb + grp * per_g);
+    const uint32_t ge = min(we, gb + per_g);
+    const uint32_t nchunks = (per_g + CH - 1) / CH;          // warp-uniform
+    uint32_t (*sl)[SW] = slots[warp][grp];
 
-    float4 acc[V];
+    float acc[V][4];
 #pragma unroll
-    for (int v = 0; v < V; ++v) acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[v][q] = 0.f;
     uint32_t cur = 0xffffffffu;
 
-    for (uint32_t j0 = gb; j0 < ge; j0 += U) {
-        float    val[U];
-        uint32_t row[U];
-        float4   y[U][N][V];
-        static_for<0, U>([&](auto uc) {
-            constexpr int u = decltype(uc)::value;
-            const bool ok = (j0 + u) < ge;
-            const uint32_t p = tl.begin + (ok ? j0 + u : gb);
-            val[u] = ok ? __ldg(in.vals + p) : 0.f;
-            row[u] = ok ? __ldg(rowcol + p) : cur;
+    // prefetch registers for one chunk
+    uint32_t pf[LPE][1 + N];
+    auto prefetch = [&](uint32_t ch) {
 #pragma unroll
-            for (int w = 0; w < N; ++w) {
-                const uint32_t id = (w == n) ? 0u : __ldg(in.idx[w] + p);
+        for (int k = 0; k < LPE; ++k) {
+            const uint32_t e = gb + ch * CH + gl + k * G;
+            const uint32_t p = tl.begin + (e < ge ? e : gb);
+            pf[k][0] = __float_as_uint(__ldg(in.vals + p));
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int c4 = gl + v * G;
-                    y[u][w][v] = (w != n && (V == 1 || c4 < C4)) ? gather4<BF>(F, w, id, Rp, c4)
-                                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-        });
-        static_for<0, U>([&](auto uc) {
-            constexpr int u = decltype(uc)::value;
-            const bool flush = (j0 + u < ge) && row[u] != cur && cur != 0xffffffffu;
-            if (flush) {
-                float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
+            for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldg(in.idx[w] + p);
+        }
+    };
+    if (nchunks) prefetch(0);
+
+    for (uint32_t ch = 0; ch < nchunks; ++ch) {
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int c4 = gl + v * G;
-                    if (V == 1 || c4 < C4) atomicAdd(out + c4, acc[v]);
-                    acc[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-            if (j0 + u < ge) cur = row[u];
-            if (j0 + u >= ge) val[u] = 0.f;
-            // non-target modes in increasing order: the first starts the
-            // product (w0), the middle ones multiply, the last (w_last) is
-            // fused into the accumulate -- the reference's order
+        for (int k = 0; k < LPE; ++k)
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-                float4 pr = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int f = 0; f < 1 + N; ++f) sl[gl + k * G][f] = pf[k][f];
+        __syncwarp();
+        if (ch + 1 < nchunks) prefetch(ch + 1);
+        const uint32_t base = gb + ch * CH;
+        const int cnt = base < ge ? (int)min((uint32_t)CH, ge - base) : 0;
+        for (int e0 = 0; e0 < cnt; e0 += U) {
+            float val[U];
+            uint32_t row[U];
+            float y[U][N][V][4];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u;
+                const uint32_t* s = sl[e < cnt ? e : 0];
+                val[u] = e < cnt ? __uint_as_float(s[0]) : 0.f;
+                row[u] = s[1 + n];
 #pragma unroll
                 for (int w = 0; w < N; ++w) {
-                    if (w == n) continue;
-                    if (w == w0)      pr = scale4(y[u][w][v], val[u]);
-                    else if (w == wl) acc[v] = fma4(pr, y[u][w][v], acc[v]);
-                    else              pr = mul4(pr, y[u][w][v]);
+                    const uint32_t id = s[1 + w];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        const int c4 = gl + v * G;
+                        float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, Rp, c4);
+                        y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
+                        y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
+                    }
                 }
-                if (wl < 0) acc[v] = add4(acc[v], pr);
             }
-        });
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (e0 + u < cnt) {
+                    if (row[u] != cur) {
+                        if (cur != 0xffffffffu) {
+                            float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
+#pragma unroll
+                            for (int v = 0; v < V; ++v) {
+                                const int c4 = gl + v * G;
+                                if (V == 1 || c4 < C4)
+                                    atomicAdd(out + c4, make_float4(acc[v][0], acc[v][1], acc[v][2], acc[v][3]));
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) acc[v][q] = 0.f;
+                            }
+                        }
+                        cur = row[u];
+                    }
+                    // non-target modes in increasing order: the first starts
+                    // the product (w0), the middle ones multiply, the last
+                    // (w_last) is fused into the accumulate (reference order)
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            // select instead of index: w0/wl are runtime values
+                            float pr = val[u], yl = 1.f;
+#pragma unroll
+                            for (int w = 0; w < N; ++w) {
+                                const float yy = y[u][w][v][q];
+                                pr = (w != n && w != wl) ? pr * yy : pr;
+                                yl = (w == wl) ? yy : yl;
+                            }
+                            acc[v][q] = (wl >= 0) ? __fmaf_rn(pr, yl, acc[v][q]) : acc[v][q] + pr;
+                        }
+                }
+            }
+        }
+        __syncwarp();
     }
     if (cur != 0xffffffffu) {
         float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             const int c4 = gl + v * G;
-            if (V == 1 || c4 < C4) atomicAdd(out + c4, acc[v]);
+            if (V == 1 || c4 < C4)
+                atomicAdd(out + c4, make_float4(acc[v][0], acc[v][1], acc[v][2], acc[v][3]));
         }
     }
 }
@@ -352,8 +406,8 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
     const SlabPtrs sp = slab_in(in, p.N);
     float* out = p.Yhat[n];
 #define DGPU_RUN(G, V)                                                                        \
-    k_mttkrp_rowrun<N, G, V, BF><<<ntiles, kRunThreads, 0, p.stream>>>(sp, in.idx[n], tiles, F, \
-                                                                       out, n, w0, wl, p.Rp)
+    k_mttkrp_rowrun<N, G, V, BF><<<ntiles, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, w0, \
+                                                                       wl, p.Rp)
     if (C4 == 4) DGPU_RUN(4, 1);
     else if (C4 == 8) DGPU_RUN(8, 1);
     else if (C4 == 16) DGPU_RUN(16, 1);

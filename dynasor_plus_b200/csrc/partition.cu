@@ -10,22 +10,26 @@
 //  This file computes the same permutation with three bandwidth-bound
 //  kernels over tiles of that sequence (tiles listed in processing order):
 //
-//    1. k_part_hist    per-tile bucket histogram  -> cnt[b * ntiles + t]
-//    2. k_scan_*       exclusive scan of cnt in bucket-major order -> off
-//                      (bucket-major order = all tiles of bucket 0, then
-//                      bucket 1, ...; so off[b][t] is the global slot of
-//                      the first element of bucket b in tile t)
+//    1. k_part_hist    per-tile bucket histogram -> cnt
+//    2. k_scan_*       exclusive scan of cnt -> off (global slot of the first
+//                      element of bucket b in tile t)
 //    3. k_part_scatter stable in-tile ranking (warp match + per-warp
 //                      counters) and the scatter of (val, idx[0..N-1]).
+//
+//  cnt layout: entry (t, b) lives at seg_first(t) * nb + b * nt_seg(t) +
+//  (t - seg_first(t)).  A global partition has one segment (seg_first = 0,
+//  nt_seg = ntiles): bucket-major, tile-minor.  A segmented partition
+//  (every super-shard sorted independently inside its own slab range, the
+//  fiber sort) has one block per shard, bucket-major inside it; since the
+//  shards' tiles are listed in slab order one flat scan yields the offsets
+//  of every segment at once.
 //
 //  Keys wider than kMaxBuckets are sorted by least-significant-digit
 //  passes; a stable LSD sort gives the same permutation as one stable
 //  counting sort on the full key.  The same machinery builds the initial
 //  mode-0 shard order (src/dynasor_preprocess.cpp:113-241) and the fiber
-//  sort (stable sort of a mode's slab by row; a stable sort by row of a
-//  slab grouped by shard equals the reference's per-shard counting sort,
-//  src/dynasor_preprocess.cpp:2225-2256, because shards are contiguous row
-//  ranges in increasing order).
+//  sort: a stable per-shard counting sort by row (src/dynasor_preprocess.cpp:
+//  471-521, 2225-2256), keyed by the row's low bits (row - shard base).
 // ============================================================================
 #include "dgpu_internal.h"
 
@@ -45,21 +49,37 @@ __device__ __forceinline__ uint32_t part_key(uint32_t v, int shift, uint32_t mas
     return (v >> shift) & mask;
 }
 
+// (segment base, tiles in segment) of tile t
+__device__ __forceinline__ void seg_of(const Tile& tl, uint32_t t, uint32_t ntiles,
+                                       const uint32_t* seg_n, uint32_t* first, uint32_t* nt) {
+    if (seg_n) {
+        *first = tl.seg_first;
+        *nt = seg_n[tl.shard];
+    } else {
+        *first = 0;
+        *nt = ntiles;
+    }
+    (void)t;
+}
+
 __global__ void __launch_bounds__(kPartThreads)
 k_part_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles,
-            uint32_t ntiles, int shift, uint32_t mask, uint32_t nb,
-            uint32_t* __restrict__ cnt)
+            uint32_t ntiles, const uint32_t* __restrict__ seg_n, int shift, uint32_t mask,
+            uint32_t nb, uint32_t* __restrict__ cnt)
 {
     extern __shared__ uint32_t h[];
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) h[b] = 0;
     __syncthreads();
-    const Tile tl = tiles[blockIdx.x];
+    const uint32_t t = blockIdx.x;
+    const Tile tl = tiles[t];
     const uint32_t* k = keycol + tl.begin;
     for (uint32_t j = threadIdx.x; j < tl.count; j += blockDim.x)
         atomicAdd(&h[part_key(__ldg(k + j), shift, mask)], 1u);
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x)
-        cnt[(size_t)b * ntiles + blockIdx.x] = h[b];
+    uint32_t first, nt;
+    seg_of(tl, t, ntiles, seg_n, &first, &nt);
+    uint32_t* c = cnt + (size_t)first * nb + (t - first);
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) c[(size_t)b * nt] = h[b];
 }
 
 // --- exclusive scan (three phases, u32) ----------------------------------
@@ -157,18 +177,22 @@ k_scan_down(const uint32_t* __restrict__ in, size_t n, const uint32_t* __restric
 
 // --- stable scatter ----------------------------------------------------------
 // One CTA per tile.  Warp w owns the w-th contiguous eighth of the tile, so
-// tile order = warp order = lane order within a 32-element step.
+// tile order = warp order = lane order within a 32-element step.  Per-warp
+// counters are 16-bit (a warp handles at most kTile / 8 elements).
+template <int N>
 __global__ void __launch_bounds__(kPartThreads)
-k_part_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out, int N, const Tile* __restrict__ tiles,
-               uint32_t ntiles, const uint32_t* __restrict__ off, int key_mode,
-               int shift, uint32_t mask, uint32_t nb)
+k_part_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
+               const Tile* __restrict__ tiles, uint32_t ntiles, const uint32_t* __restrict__ seg_n,
+               const uint32_t* __restrict__ off, int key_mode, int shift, uint32_t mask,
+               uint32_t nb)
 {
-    extern __shared__ uint32_t wcnt[];   // [kPartWarps][nb]
+    extern __shared__ uint32_t wcnt[];   // [kPartWarps][nb] running slots
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t i = threadIdx.x; i < kPartWarps * nb; i += blockDim.x) wcnt[i] = 0;
     __syncthreads();
 
-    const Tile tl = tiles[blockIdx.x];
+    const uint32_t t = blockIdx.x;
+    const Tile tl = tiles[t];
     const uint32_t per = (tl.count + kPartWarps - 1) / kPartWarps;
     const uint32_t wb = min(tl.count, (uint32_t)warp * per);
     const uint32_t we = min(tl.count, wb + per);
@@ -179,8 +203,11 @@ k_part_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Slab
         atomicAdd(&my[part_key(__ldg(kc + j), shift, mask)], 1u);
     __syncthreads();
 
+    uint32_t first, nt;
+    seg_of(tl, t, ntiles, seg_n, &first, &nt);
+    const uint32_t* o = off + (size_t)first * nb + (t - first);
     for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
-        uint32_t run = off[(size_t)b * ntiles + blockIdx.x];
+        uint32_t run = o[(size_t)b * nt];
 #pragma unroll
         for (int w = 0; w < kPartWarps; ++w) {
             const uint32_t c = wcnt[(size_t)w * nb + b];
@@ -205,6 +232,7 @@ k_part_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Slab
             if (rank == 0) my[key] = start + __popc(peers);
             const uint32_t dst = start + rank;
             out.vals[dst] = __ldg(in.vals + src);
+#pragma unroll
             for (int w = 0; w < N; ++w) out.idx[w][dst] = __ldg(in.idx[w] + src);
         }
         __syncwarp();
@@ -239,11 +267,30 @@ int exclusive_scan(Plan& p, const uint32_t* in, size_t n, uint32_t* out, uint32_
     return DGPU_OK;
 }
 
+template <int N>
+int launch_scatter(Plan& p, const Slab& in, const Slab& out, const Tile* tiles, uint32_t ntiles,
+                   const uint32_t* seg_n, int key_mode, int key_shift, uint32_t key_mask,
+                   uint32_t nb)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        DGPU_CUDA(cudaFuncSetAttribute(k_part_scatter<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(kPartWarps * kMaxBuckets * sizeof(uint32_t))));
+        attr_set = true;
+    }
+    const size_t ssm = (size_t)kPartWarps * nb * sizeof(uint32_t);
+    k_part_scatter<N><<<ntiles, kPartThreads, ssm, p.stream>>>(
+        slab_in(in, p.N), slab_out(out, p.N), tiles, ntiles, seg_n, p.part_off, key_mode,
+        key_shift, key_mask, nb);
+    DGPU_CUDA(cudaGetLastError());
+    return DGPU_OK;
+}
+
 }  // namespace
 
 int stable_partition(Plan& p, const Slab& in, const Tile* tiles, uint32_t ntiles,
                      int key_mode, int key_shift, uint32_t key_mask, uint32_t nb,
-                     const Slab& out)
+                     const Slab& out, const uint32_t* seg_n)
 {
     if (ntiles == 0) return DGPU_OK;
     if (nb == 0 || nb > kMaxBuckets) {
@@ -257,7 +304,7 @@ int stable_partition(Plan& p, const Slab& in, const Tile* tiles, uint32_t ntiles
     {
         LaunchTimer t(p, KK_PART_HIST, elem * 4.0 + (double)entries * 4.0);
         const size_t hsm = nb * sizeof(uint32_t);
-        k_part_hist<<<ntiles, kPartThreads, hsm, p.stream>>>(in.idx[key_mode], tiles, ntiles,
+        k_part_hist<<<ntiles, kPartThreads, hsm, p.stream>>>(in.idx[key_mode], tiles, ntiles, seg_n,
                                                              key_shift, key_mask, nb, p.part_cnt);
         DGPU_CUDA(cudaGetLastError());
     }
@@ -267,19 +314,16 @@ int stable_partition(Plan& p, const Slab& in, const Tile* tiles, uint32_t ntiles
     }
     {
         LaunchTimer t(p, KK_PART_SCATTER, elem * 2.0 * row_bytes + (double)entries * 4.0);
-        const size_t ssm = (size_t)kPartWarps * nb * sizeof(uint32_t);
-        static bool attr_set = false;   // per process; the kernel is per device-agnostic
-        if (!attr_set) {
-            DGPU_CUDA(cudaFuncSetAttribute(k_part_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(kPartWarps * kMaxBuckets * sizeof(uint32_t))));
-            attr_set = true;
+        switch (p.N) {
+#define DGPU_SC(NN) case NN: return launch_scatter<NN>(p, in, out, tiles, ntiles, seg_n, key_mode, \
+                                                    key_shift, key_mask, nb)
+            DGPU_SC(2); DGPU_SC(3); DGPU_SC(4); DGPU_SC(5); DGPU_SC(6); DGPU_SC(7); DGPU_SC(8);
+#undef DGPU_SC
+            default:
+                set_error("stable_partition: %d modes unsupported", p.N);
+                return DGPU_ERR_ARG;
         }
-        k_part_scatter<<<ntiles, kPartThreads, ssm, p.stream>>>(
-            slab_in(in, p.N), slab_out(out, p.N), p.N, tiles, ntiles, p.part_off, key_mode,
-            key_shift, key_mask, nb);
-        DGPU_CUDA(cudaGetLastError());
     }
-    return DGPU_OK;
 }
 
 int stable_sort_pingpong(Plan& p, int a, int b, const Tile* tiles, uint32_t ntiles,
@@ -309,6 +353,31 @@ int stable_sort_pingpong(Plan& p, int a, int b, const Tile* tiles, uint32_t ntil
         std::swap(src, dst);
     }
     *result = src;
+    return DGPU_OK;
+}
+
+// Per-shard stable sort of mode n's slab by row: segmented LSD passes over
+// the row's low shift_n bits (the row's offset inside its shard).
+int fiber_sort(Plan& p, int n, int src, int other, int* result) {
+    const int bits = p.shift[n];
+    *result = src;
+    if (bits == 0) return DGPU_OK;               // one row per shard: already sorted
+    if (!p.ftiles_d[n]) {
+        set_error("fiber_sort: mode %d has no fiber tiles", n);
+        return DGPU_ERR_NOT_BUILT;
+    }
+    const int passes = (bits + kDigitBits - 1) / kDigitBits;
+    const int dbits = (bits + passes - 1) / passes;
+    int a = src, b = other;
+    for (int k = 0; k < passes; ++k) {
+        const int sh = k * dbits;
+        const int hi = std::min(bits, sh + dbits);
+        const uint32_t mask = (1u << (hi - sh)) - 1u;
+        DGPU_TRY(stable_partition(p, p.slab[a], p.ftiles_d[n], p.nftiles[n], n, sh, mask, mask + 1,
+                                  p.slab[b], p.fseg_d[n]));
+        std::swap(a, b);
+    }
+    *result = a;
     return DGPU_OK;
 }
 

@@ -150,6 +150,8 @@ Plan::~Plan() {
     for (auto& s : slab) dev_free(s.raw);
     for (int n = 0; n < kMaxModes; ++n) {
         dev_free(tiles_d[n]);
+        dev_free(ftiles_d[n]);
+        dev_free(fseg_d[n]);
         dev_free(Y[n]);
         dev_free(Yhat[n]);
         dev_free(Yb[n]);
@@ -263,7 +265,7 @@ static void build_tiles(Plan& p) {
                     tl.begin = (uint32_t)x;
                     tl.count = (uint32_t)std::min<uint64_t>(kTile, e - x);
                     tl.shard = s;
-                    tl.pad = 0;
+                    tl.seg_first = 0;
                     v.push_back(tl);
                 }
             }
@@ -275,6 +277,33 @@ static int upload_tiles(Plan& p, const std::vector<Tile>& h, Tile** d) {
     if (!h.empty())
         DGPU_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(Tile),
                                   cudaMemcpyHostToDevice, p.stream));
+    return DGPU_OK;
+}
+
+// Tiles of mode n in slab order (shard 0, 1, ...) with their segment
+// bookkeeping, for the per-shard fiber sort.
+static int build_fiber_tiles(Plan& p, int n) {
+    std::vector<Tile> v;
+    std::vector<uint32_t> seg(p.K[n], 0);
+    for (uint32_t s = 0; s < p.K[n]; ++s) {
+        const uint64_t b = p.sbeg[n][s], e = p.send[n][s];
+        const uint32_t first = (uint32_t)v.size();
+        for (uint64_t x = b; x < e; x += kTile) {
+            Tile tl;
+            tl.begin = (uint32_t)x;
+            tl.count = (uint32_t)std::min<uint64_t>(kTile, e - x);
+            tl.shard = s;
+            tl.seg_first = first;
+            v.push_back(tl);
+        }
+        seg[s] = (uint32_t)v.size() - first;
+    }
+    p.nftiles[n] = (uint32_t)v.size();
+    DGPU_TRY(upload_tiles(p, v, &p.ftiles_d[n]));
+    DGPU_TRY(dev_alloc(p, (void**)&p.fseg_d[n], std::max<size_t>(1, seg.size()) * 4));
+    DGPU_CUDA(cudaMemcpyAsync(p.fseg_d[n], seg.data(), seg.size() * 4, cudaMemcpyHostToDevice,
+                              p.stream));
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
     return DGPU_OK;
 }
 
@@ -379,6 +408,8 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     build_schedule(p);
     build_tiles(p);
     for (int n = 0; n < p.N; ++n) DGPU_TRY(upload_tiles(p, p.tiles_h[n], &p.tiles_d[n]));
+    for (int n = 0; n < p.N; ++n)
+        if (p.fiber && p.kclass[n] == 2) DGPU_TRY(build_fiber_tiles(p, n));
     {
         std::vector<Tile> id;
         for (uint64_t x = 0; x < p.nnz; x += kTile) {
@@ -386,7 +417,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
             tl.begin = (uint32_t)x;
             tl.count = (uint32_t)std::min<uint64_t>(kTile, p.nnz - x);
             tl.shard = 0;
-            tl.pad = 0;
+            tl.seg_first = 0;
             id.push_back(tl);
         }
         p.n_ident_tiles = (uint32_t)id.size();
@@ -423,8 +454,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
             for (int k = 0; k < p.N; ++k) {
                 if (p.kclass[k] != 2) continue;
                 int r = 0;
-                DGPU_TRY(stable_sort_pingpong(p, k, p.N, p.ident_tiles_d, p.n_ident_tiles, k, 0,
-                                              p.dims[k], &r));
+                DGPU_TRY(fiber_sort(p, k, k, p.N, &r));
                 if (r != k)
                     DGPU_CUDA(cudaMemcpyAsync(p.slab[k].raw, p.slab[r].raw, p.slab[k].bytes,
                                               cudaMemcpyDeviceToDevice, p.stream));
@@ -461,8 +491,7 @@ int mode_pingpong(Plan& p, int n) {
     const int other = 1 - p.cur;
     if (p.fiber && p.kclass[n] == 2) {
         int r = 0;
-        DGPU_TRY(stable_sort_pingpong(p, p.cur, other, p.ident_tiles_d, p.n_ident_tiles, n, 0,
-                                      p.dims[n], &r));
+        DGPU_TRY(fiber_sort(p, n, p.cur, other, &r));
         p.cur = r;
     }
     {
