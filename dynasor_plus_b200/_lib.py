@@ -103,6 +103,8 @@ _SIGS = {
     "dgpu_tensor_norm_sq": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "dgpu_model_values": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dgpu_cpopt_gradient": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dgpu_sort_slab_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_uint32]),
     "dgpu_load_coo_tensor": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Coo)]),
     "dgpu_load_tns": (C.c_int, [C.c_char_p, C.POINTER(Coo)]),
     "dgpu_load_dnb": (C.c_int, [C.c_char_p, C.POINTER(Coo)]),

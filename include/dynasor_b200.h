@@ -224,6 +224,28 @@ int dgpu_model_values(dgpu_plan* plan, float* model_host);
  * written to host I_n x Rp FP32 buffers. */
 int dgpu_cpopt_gradient(dgpu_plan* plan, float* const* grad_host);
 
+/* ---- allocation-free stable shard partition (no counterpart in the
+ *      reference: an addition for callers that may not allocate device
+ *      memory, e.g. code whose device memory is owned by a host framework's
+ *      pool, or latency-critical paths where cudaMalloc's device-wide
+ *      synchronisation is not allowed) ------------------------------------
+ * Stable counting sort of a device SoA slab, taken in slab order, by key =
+ * idx[key_mode][i] >> key_shift (< num_buckets <= 2048), from
+ * (vals_in, idx_in[]) into (vals_out, idx_out[]) -- the partition the remap
+ * and the initial mode-0 shard order use.  idx_in/idx_out are host arrays
+ * of num_modes device pointers.  Allocates nothing: its scratch is one fixed
+ * 16 MiB device array that every GPU loading the library holds until exit;
+ * requests needing more than 2,095,104 counters (num_buckets *
+ * ceil(nnz / 4096)) are rejected with DGPU_ERR_ARG.  Calls share that
+ * array, so calls whose device work overlaps race; the first call on a
+ * device resolves the array's address and should come before any stream
+ * capture.  Waits for `stream` before returning; a key >= num_buckets
+ * yields DGPU_ERR_INDEX. */
+int dgpu_sort_slab_noalloc(void* stream, int num_modes, uint64_t nnz,
+                           const float* vals_in, const uint32_t* const* idx_in,
+                           float* vals_out, uint32_t* const* idx_out,
+                           int key_mode, int key_shift, uint32_t num_buckets);
+
 /* ---- host loaders (replace load_coo_tensor / save_dnb_tensor /
  *      dump_factor_matrix_bin, src/dynasor_io.cpp:576-1348) ---------------- */
 /* A host COO tensor owned by the library (free with dgpu_coo_free). */
