@@ -68,6 +68,35 @@ struct Tile {
     uint32_t seg_first;
 };
 
+// A chunk: consecutive entries [tile_begin, tile_end) of a tile list, all in
+// one segment.  One CTA of the partition kernels handles one chunk.
+struct Chunk {
+    uint32_t tile_begin;
+    uint32_t tile_end;
+    uint32_t seg;
+    uint32_t pad;
+};
+
+// A segment: chunks [chunk_begin, chunk_end) sorted as one independent
+// counting sort whose output starts at slab position `base`.
+struct Seg {
+    uint32_t chunk_begin;
+    uint32_t chunk_end;
+    uint32_t base;
+    uint32_t pad;
+};
+
+// A tile list prepared for the chunked partition (device arrays).
+struct PartList {
+    Tile*    tiles = nullptr;
+    uint32_t ntiles = 0;
+    Chunk*   chunks = nullptr;
+    uint32_t nchunks = 0;
+    Seg*     segs = nullptr;
+    uint32_t nsegs = 0;
+    bool     own_tiles = false;
+};
+
 // SoA slab on the device.
 struct Slab {
     void*     raw = nullptr;
@@ -142,21 +171,20 @@ struct Plan {
     Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for
-    Tile*        tiles_d[kMaxModes] = {nullptr};
-    Tile*        ftiles_d[kMaxModes] = {nullptr};  // slab-order tiles per shard (fiber sort)
-    uint32_t*    fseg_d[kMaxModes] = {nullptr};    // tiles per shard, [K_n]
-    uint32_t     nftiles[kMaxModes] = {};
-    Tile*        ident_tiles_d = nullptr;       // identity order over [0, nnz)
-    uint32_t     n_ident_tiles = 0;
+    Tile*        tiles_d[kMaxModes] = {nullptr};   // mode n tiles, processing order
+    PartList     proc[kMaxModes];               // remap of mode n (global, processing order)
+    PartList     fib[kMaxModes];                // fiber sort of mode n (segmented by shard)
+    PartList     ident;                         // identity order over [0, nnz) (global)
+    int          sms = 148;                     // SM count of the device
     float*       Y[kMaxModes] = {nullptr};
     float*       Yhat[kMaxModes] = {nullptr};
     __nv_bfloat16* Yb[kMaxModes] = {nullptr};
     bool         yb_stale[kMaxModes] = {};
-    uint32_t*    part_cnt = nullptr;            // [buckets * tiles]
-    uint32_t*    part_off = nullptr;            // [buckets * tiles]
-    size_t       part_cap = 0;                  // entries
-    uint32_t*    scan_aux = nullptr;            // block sums for the scan
-    size_t       scan_aux_cap = 0;
+    uint32_t*    part_cnt = nullptr;            // [chunks x buckets] counts
+    uint32_t*    part_off = nullptr;            // [chunks x buckets] in-segment prefixes
+    size_t       part_cap = 0;                  // entries of each
+    uint32_t*    part_base = nullptr;           // [segments x buckets] bucket starts
+    size_t       part_base_cap = 0;
     int*         err_flag = nullptr;            // device-side fault flag
     float*       lambda = nullptr;              // [Rp]
     double*      la_work = nullptr;             // CP-ALS R x R scratch (FP64)
@@ -196,19 +224,26 @@ int launch_shard_counts(Plan& p, const Slab& s, uint64_t* counts_d, size_t total
 // written to `out` ordered by key = (idx[key_mode] >> key_shift) & key_mask
 // (buckets < nb <= kMaxBuckets), each bucket starting at `base_off` +
 // (elements of all smaller buckets), stably.  Uses p.part_cnt/part_off.
-// With `seg_n` (tiles per shard, indexed by Tile::shard) the partition is
-// segmented: every shard is sorted independently inside its own range.
-int stable_partition(Plan& p, const Slab& in, const Tile* tiles, uint32_t ntiles,
+// The list's segments are sorted independently (a global list has one).
+int stable_partition(Plan& p, const Slab& in, const PartList& list,
                      int key_mode, int key_shift, uint32_t key_mask, uint32_t nb,
-                     const Slab& out, const uint32_t* seg_n = nullptr);
+                     const Slab& out);
 // Fiber sort of mode n (stable sort of every mode-n shard by row) from
 // slab[src] ping-ponging with slab[other]; *result = slab holding it.
 int fiber_sort(Plan& p, int n, int src, int other, int* result);
-// Stable sort of the sequence listed by `tiles` over slab[a] by the key
-// (idx[key_mode] >> key_shift) < key_limit, any key range: one partition
-// pass per least-significant digit, ping-ponging between slab[a] and
-// slab[b]; *result receives the slab index that holds the sorted data.
-int stable_sort_pingpong(Plan& p, int a, int b, const Tile* tiles, uint32_t ntiles,
+// Build the chunk/segment tables of a tile list.  `seg_of_tile` (host, may
+// be empty) gives each tile's segment and `seg_base` each segment's output
+// start; empty means one global segment starting at 0.
+int build_partlist(Plan& p, const std::vector<Tile>& tiles,
+                   const std::vector<uint32_t>& seg_of_tile,
+                   const std::vector<uint32_t>& seg_base, PartList& out, Tile* shared_tiles);
+void free_partlist(PartList& l);
+// Stable sort of the sequence listed by `first` (a global list) over slab[a]
+// by the key (idx[key_mode] >> key_shift) < key_limit, any key range: one
+// partition pass per least-significant digit (later passes in slab order),
+// ping-ponging between slab[a] and slab[b]; *result receives the slab index
+// that holds the sorted data.
+int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first,
                          int key_mode, int key_shift, uint64_t key_limit, int* result);
 
 // MTTKRP of mode n over the tiles of the slab `in` into p.Yhat[n].

@@ -105,18 +105,27 @@ struct RunBatch {
 // shared slot array (prefetching the next chunk into registers), then walk
 // the chunk U nonzeros at a time: U x (N-1) float4 gathers in flight per
 // lane, products in registers, one vector atomic per finished row run.
-template <int N, int G, int V, bool BF>
-__global__ void __launch_bounds__(kRunThreads, 3)
+// TN >= 0 pins the target mode at compile time (the reference's TGT
+// specialisation, src/dynasor_kernel.cpp:247-265), so only the N-1 gathered
+// rows occupy registers; TN = -1 takes the mode at run time.
+template <int N, int G, int V, bool BF, int TN>
+__global__ void __launch_bounds__(kRunThreads, 2)
 k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ tiles,
                 const __grid_constant__ FacPtrs F, float* __restrict__ Yhat,
-                int n, int w0, int wl, int Rp)
+                int n_rt, int w0_rt, int wl_rt, int Rp)
 {
+    const int n = TN >= 0 ? TN : n_rt;
+    const int w0 = TN >= 0 ? (TN == 0 ? 1 : 0) : w0_rt;
+    const int wl = TN >= 0 ? (N == 2 ? -1 : (TN == N - 1 ? N - 2 : N - 1)) : wl_rt;
     constexpr int U = RunBatch<N, V>::U;
     constexpr int NG = 32 / G;                    // groups per warp
-    constexpr int CH = G >= 16 ? G : 16;          // nonzeros staged per group per chunk
+    constexpr int CH = G >= 16 ? G : ((1 + N + 3) / 4 * 4 > 8 ? 8 : 16);  // staged per group
     constexpr int LPE = CH / G;                   // nonzeros loaded per lane per chunk
-    constexpr int SW = (1 + N + 3) / 4 * 4;       // words per slot
-    __shared__ uint32_t slots[kRunWarps][NG][CH][SW];
+    constexpr int SW = (1 + N + 3) / 4 * 4;       // words per slot (16-byte multiple)
+    // Group slot areas are CH*SW + 4 words apart so the NG groups' 16-byte
+    // slot reads of one instruction land in distinct banks.
+    constexpr int GS = CH * SW + 4;
+    __shared__ __align__(16) uint32_t slots[kRunWarps * NG * GS];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / G, gl = lane % G;
@@ -130,7 +139,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     const uint32_t gb = min(we, wb + grp * per_g);
     const uint32_t ge = min(we, gb + per_g);
     const uint32_t nchunks = (per_g + CH - 1) / CH;          // warp-uniform
-    uint32_t (*sl)[SW] = slots[warp][grp];
+    uint32_t* gs = slots + (warp * NG + grp) * GS;
 
     float acc[V][4];
 #pragma unroll
@@ -140,7 +149,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     uint32_t cur = 0xffffffffu;
 
     // prefetch registers for one chunk
-    uint32_t pf[LPE][1 + N];
+    uint32_t pf[LPE][SW];
     auto prefetch = [&](uint32_t ch) {
 #pragma unroll
         for (int k = 0; k < LPE; ++k) {
@@ -149,6 +158,8 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
             pf[k][0] = __float_as_uint(__ldg(in.vals + p));
 #pragma unroll
             for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldg(in.idx[w] + p);
+#pragma unroll
+            for (int f = 1 + N; f < SW; ++f) pf[k][f] = 0u;
         }
     };
     if (nchunks) prefetch(0);
@@ -157,7 +168,9 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
 #pragma unroll
         for (int k = 0; k < LPE; ++k)
 #pragma unroll
-            for (int f = 0; f < 1 + N; ++f) sl[gl + k * G][f] = pf[k][f];
+            for (int f = 0; f < SW; f += 4)
+                *reinterpret_cast<uint4*>(gs + (gl + k * G) * SW + f) =
+                    make_uint4(pf[k][f], pf[k][f + 1], pf[k][f + 2], pf[k][f + 3]);
         __syncwarp();
         if (ch + 1 < nchunks) prefetch(ch + 1);
         const uint32_t base = gb + ch * CH;
@@ -169,9 +182,16 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int e = e0 + u;
-                const uint32_t* s = sl[e < cnt ? e : 0];
+                uint32_t s[SW];
+#pragma unroll
+                for (int f = 0; f < SW; f += 4) {
+                    const uint4 q = *reinterpret_cast<const uint4*>(gs + (e < cnt ? e : 0) * SW + f);
+                    s[f] = q.x; s[f + 1] = q.y; s[f + 2] = q.z; s[f + 3] = q.w;
+                }
                 val[u] = e < cnt ? __uint_as_float(s[0]) : 0.f;
-                row[u] = s[1 + n];
+                row[u] = 0u;
+#pragma unroll
+                for (int w = 0; w < N; ++w) row[u] = (w == n) ? s[1 + w] : row[u];
 #pragma unroll
                 for (int w = 0; w < N; ++w) {
                     const uint32_t id = s[1 + w];
@@ -405,13 +425,26 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
     const int C4 = p.Rp / 4;
     const SlabPtrs sp = slab_in(in, p.N);
     float* out = p.Yhat[n];
-#define DGPU_RUN(G, V)                                                                        \
-    k_mttkrp_rowrun<N, G, V, BF><<<ntiles, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, w0, \
-                                                                       wl, p.Rp)
-    if (C4 == 4) DGPU_RUN(4, 1);
-    else if (C4 == 8) DGPU_RUN(8, 1);
-    else if (C4 == 16) DGPU_RUN(16, 1);
-    else if (C4 == 32) DGPU_RUN(32, 1);
+#define DGPU_RUNT(G, V, TN)                                                                      \
+    k_mttkrp_rowrun<N, G, V, BF, TN><<<ntiles, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, \
+                                                                           w0, wl, p.Rp)
+#define DGPU_RUN(G, V) DGPU_RUNT(G, V, -1)
+    // target-mode specialisations for the common 3- and 4-mode, Rp <= 128 shapes
+#define DGPU_RUN_TGT(G)                                                       \
+    do {                                                                      \
+        if constexpr (N == 3 || N == 4) {                                     \
+            if (n == 0) DGPU_RUNT(G, 1, 0);                                   \
+            else if (n == 1) DGPU_RUNT(G, 1, 1);                              \
+            else if (n == 2) DGPU_RUNT(G, 1, 2);                              \
+            else DGPU_RUNT(G, 1, (N == 4 ? 3 : -1));                          \
+        } else {                                                              \
+            DGPU_RUN(G, 1);                                                   \
+        }                                                                     \
+    } while (0)
+    if (C4 == 4) DGPU_RUN_TGT(4);
+    else if (C4 == 8) DGPU_RUN_TGT(8);
+    else if (C4 == 16) DGPU_RUN_TGT(16);
+    else if (C4 == 32) DGPU_RUN_TGT(32);
     else if (C4 <= 64) DGPU_RUN(32, 2);
     else if (C4 <= 96) DGPU_RUN(32, 3);
     else if (C4 <= 128) DGPU_RUN(32, 4);
@@ -420,7 +453,9 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
         set_error("mttkrp: rank_padded %d exceeds the supported maximum 1024", p.Rp);
         return DGPU_ERR_ARG;
     }
+#undef DGPU_RUN_TGT
 #undef DGPU_RUN
+#undef DGPU_RUNT
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
 }

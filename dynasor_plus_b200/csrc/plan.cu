@@ -28,8 +28,6 @@
 
 namespace dgpu {
 
-int stable_sort_pingpong(Plan& p, int a, int b, const Tile* tiles, uint32_t ntiles,
-                         int key_mode, int key_shift, uint64_t key_limit, int* result);
 
 // ----------------------------------------------------------------------------
 //  errors
@@ -149,17 +147,17 @@ Plan::~Plan() {
     for (auto e : event_pool) cudaEventDestroy(e);
     for (auto& s : slab) dev_free(s.raw);
     for (int n = 0; n < kMaxModes; ++n) {
+        free_partlist(proc[n]);
+        free_partlist(fib[n]);
         dev_free(tiles_d[n]);
-        dev_free(ftiles_d[n]);
-        dev_free(fseg_d[n]);
         dev_free(Y[n]);
         dev_free(Yhat[n]);
         dev_free(Yb[n]);
     }
-    dev_free(ident_tiles_d);
+    free_partlist(ident);
     dev_free(part_cnt);
     dev_free(part_off);
-    dev_free(scan_aux);
+    dev_free(part_base);
     dev_free(err_flag);
     dev_free(lambda);
     dev_free(la_work);
@@ -284,9 +282,10 @@ static int upload_tiles(Plan& p, const std::vector<Tile>& h, Tile** d) {
 // bookkeeping, for the per-shard fiber sort.
 static int build_fiber_tiles(Plan& p, int n) {
     std::vector<Tile> v;
-    std::vector<uint32_t> seg(p.K[n], 0);
+    std::vector<uint32_t> seg_of, base(p.K[n], 0);
     for (uint32_t s = 0; s < p.K[n]; ++s) {
         const uint64_t b = p.sbeg[n][s], e = p.send[n][s];
+        base[s] = (uint32_t)b;
         const uint32_t first = (uint32_t)v.size();
         for (uint64_t x = b; x < e; x += kTile) {
             Tile tl;
@@ -295,16 +294,10 @@ static int build_fiber_tiles(Plan& p, int n) {
             tl.shard = s;
             tl.seg_first = first;
             v.push_back(tl);
+            seg_of.push_back(s);
         }
-        seg[s] = (uint32_t)v.size() - first;
     }
-    p.nftiles[n] = (uint32_t)v.size();
-    DGPU_TRY(upload_tiles(p, v, &p.ftiles_d[n]));
-    DGPU_TRY(dev_alloc(p, (void**)&p.fseg_d[n], std::max<size_t>(1, seg.size()) * 4));
-    DGPU_CUDA(cudaMemcpyAsync(p.fseg_d[n], seg.data(), seg.size() * 4, cudaMemcpyHostToDevice,
-                              p.stream));
-    DGPU_CUDA(cudaStreamSynchronize(p.stream));
-    return DGPU_OK;
+    return build_partlist(p, v, seg_of, base, p.fib[n], nullptr);
 }
 
 // ----------------------------------------------------------------------------
@@ -326,6 +319,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
         DGPU_CUDA(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
         p.own_stream = true;
     }
+    DGPU_CUDA(cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, p.device));
 
     // geometry
     for (int n = 0; n < p.N; ++n) {
@@ -407,7 +401,11 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     }
     build_schedule(p);
     build_tiles(p);
-    for (int n = 0; n < p.N; ++n) DGPU_TRY(upload_tiles(p, p.tiles_h[n], &p.tiles_d[n]));
+    static const std::vector<uint32_t> kNone;
+    for (int n = 0; n < p.N; ++n) {
+        DGPU_TRY(upload_tiles(p, p.tiles_h[n], &p.tiles_d[n]));
+        DGPU_TRY(build_partlist(p, p.tiles_h[n], kNone, kNone, p.proc[n], p.tiles_d[n]));
+    }
     for (int n = 0; n < p.N; ++n)
         if (p.fiber && p.kclass[n] == 2) DGPU_TRY(build_fiber_tiles(p, n));
     {
@@ -420,14 +418,12 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
             tl.seg_first = 0;
             id.push_back(tl);
         }
-        p.n_ident_tiles = (uint32_t)id.size();
-        DGPU_TRY(upload_tiles(p, id, &p.ident_tiles_d));
+        DGPU_TRY(build_partlist(p, id, kNone, kNone, p.ident, nullptr));
     }
 
     // stable scatter of the input order into mode-0 shard order
     int res = 0;
-    DGPU_TRY(stable_sort_pingpong(p, in_slab, 0, p.ident_tiles_d, p.n_ident_tiles, 0,
-                                  p.shift[0], p.K[0], &res));
+    DGPU_TRY(stable_sort_pingpong(p, in_slab, 0, p.ident, 0, p.shift[0], p.K[0], &res));
     p.cur = res;
     p.next_mode = 0;
 
@@ -443,9 +439,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
             DGPU_CUDA(cudaMemcpyAsync(p.slab[k].raw, p.slab[k - 1].raw, p.slab[k].bytes,
                                       cudaMemcpyDeviceToDevice, p.stream));
             int r = 0;
-            DGPU_TRY(stable_sort_pingpong(p, k, p.N, p.tiles_d[k - 1],
-                                          (uint32_t)p.tiles_h[k - 1].size(), k, p.shift[k],
-                                          p.K[k], &r));
+            DGPU_TRY(stable_sort_pingpong(p, k, p.N, p.proc[k - 1], k, p.shift[k], p.K[k], &r));
             if (r != k)
                 DGPU_CUDA(cudaMemcpyAsync(p.slab[k].raw, p.slab[r].raw, p.slab[k].bytes,
                                           cudaMemcpyDeviceToDevice, p.stream));
@@ -502,8 +496,7 @@ int mode_pingpong(Plan& p, int n) {
     DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
     const int nm = (n + 1) % p.N;
     int r = 0;
-    DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.tiles_d[n],
-                                  (uint32_t)p.tiles_h[n].size(), nm, p.shift[nm], p.K[nm], &r));
+    DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
     p.cur = r;
     p.next_mode = nm;
     return DGPU_OK;
