@@ -170,7 +170,7 @@ int dgpu_plan_set_stream(dgpu_plan* plan, void* stream) {
 int dgpu_plan_sync(dgpu_plan* plan) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
-    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    DGPU_TRY(sync_checked(*p));
     return DGPU_OK;
 }
 
@@ -189,7 +189,8 @@ int dgpu_plan_get_timing(dgpu_plan* plan, dgpu_kernel_timing* out, int max, int*
     if (!count || (max > 0 && !out)) { set_error("dgpu_plan_get_timing: null"); return DGPU_ERR_ARG; }
     DGPU_TRY(timing_collect(*p));
     static const char* names[KK_COUNT] = {"mttkrp", "part_hist", "part_scan", "part_scatter",
-                                          "zero", "linalg"};
+                                          "zero", "linalg", "fiber_hist", "fiber_scan",
+                                          "fiber_scatter"};
     int k = 0;
     for (int i = 0; i < KK_COUNT && k < max; ++i) {
         std::memset(&out[k], 0, sizeof(out[k]));
@@ -248,7 +249,7 @@ int dgpu_download_factor(dgpu_plan* plan, int n, float* Y) {
     if (!Y) { set_error("dgpu_download_factor: null"); return DGPU_ERR_ARG; }
     DGPU_CUDA(cudaMemcpyAsync(Y, p->Y[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
                               cudaMemcpyDeviceToHost, p->stream));
-    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    DGPU_TRY(sync_checked(*p));
     return DGPU_OK;
 }
 
@@ -259,7 +260,7 @@ int dgpu_download_yhat(dgpu_plan* plan, int n, float* Yhat) {
     if (!Yhat) { set_error("dgpu_download_yhat: null"); return DGPU_ERR_ARG; }
     DGPU_CUDA(cudaMemcpyAsync(Yhat, p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
                               cudaMemcpyDeviceToHost, p->stream));
-    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    DGPU_TRY(sync_checked(*p));
     return DGPU_OK;
 }
 
@@ -318,11 +319,8 @@ int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y, float* const*
             rc = (cudaMemcpyAsync(Yhat[n], p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
                                   cudaMemcpyDeviceToHost, p->stream) == cudaSuccess)
                      ? DGPU_OK : DGPU_ERR_CUDA;
-        cudaError_t e = cudaStreamSynchronize(p->stream);
-        if (e != cudaSuccess) {
-            set_error("dgpu_mttkrp_sweep_host: %s", cudaGetErrorString(e));
-            rc = DGPU_ERR_CUDA;
-        }
+        const int rs = sync_checked(*p);
+        if (rc == DGPU_OK) rc = rs;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         if (secs) *secs = ms * 1e-3;
@@ -343,7 +341,7 @@ int dgpu_download_slab(dgpu_plan* plan, float* vals, uint32_t* const* idx) {
         DGPU_CUDA(cudaMemcpyAsync(idx[n], s.idx[n], p->nnz * sizeof(uint32_t),
                                   cudaMemcpyDeviceToHost, p->stream));
     }
-    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    DGPU_TRY(sync_checked(*p));
     return DGPU_OK;
 }
 
@@ -360,7 +358,7 @@ int dgpu_download_copy(dgpu_plan* plan, int k, float* vals, uint32_t* const* idx
     for (int n = 0; n < p->N; ++n)
         DGPU_CUDA(cudaMemcpyAsync(idx[n], s.idx[n], p->nnz * sizeof(uint32_t),
                                   cudaMemcpyDeviceToHost, p->stream));
-    DGPU_CUDA(cudaStreamSynchronize(p->stream));
+    DGPU_TRY(sync_checked(*p));
     return DGPU_OK;
 }
 

@@ -88,13 +88,14 @@ struct Seg {
 
 // A tile list prepared for the chunked partition (device arrays).
 struct PartList {
-    Tile*    tiles = nullptr;
-    uint32_t ntiles = 0;
-    Chunk*   chunks = nullptr;
-    uint32_t nchunks = 0;
-    Seg*     segs = nullptr;
-    uint32_t nsegs = 0;
-    bool     own_tiles = false;
+    Tile*     tiles = nullptr;
+    uint32_t  ntiles = 0;
+    Chunk*    chunks = nullptr;
+    uint32_t  nchunks = 0;
+    Seg*      segs = nullptr;
+    uint32_t  nsegs = 0;
+    uint32_t* order = nullptr;    // chunk ids, largest first: the scatter's work queue
+    bool      own_tiles = false;
 };
 
 // SoA slab on the device.
@@ -118,12 +119,15 @@ struct SlabOut {
 // Kernel classes tracked by the optional per-launch CUDA-event timer.
 enum KernelKind : int {
     KK_MTTKRP = 0,       // mode-n MTTKRP
-    KK_PART_HIST = 1,    // partition: per-tile histograms
-    KK_PART_SCAN = 2,    // partition: exclusive scan
-    KK_PART_SCATTER = 3, // partition: stable scatter
+    KK_PART_HIST = 1,    // remap / shard sort partition: per-chunk histograms
+    KK_PART_SCAN = 2,    // remap / shard sort partition: exclusive scans
+    KK_PART_SCATTER = 3, // remap / shard sort partition: stable scatter
     KK_ZERO = 4,         // Yhat zeroing
     KK_LINALG = 5,       // CP-ALS dense kernels
-    KK_COUNT = 6
+    KK_FIB_HIST = 6,     // fiber sort partition: histograms
+    KK_FIB_SCAN = 7,     // fiber sort partition: scans
+    KK_FIB_SCATTER = 8,  // fiber sort partition: scatter
+    KK_COUNT = 9
 };
 
 struct TimedLaunch {
@@ -176,6 +180,9 @@ struct Plan {
     PartList     fib[kMaxModes];                // fiber sort of mode n (segmented by shard)
     PartList     ident;                         // identity order over [0, nnz) (global)
     int          sms = 148;                     // SM count of the device
+    int          part_fiber = 0;                // 1 while a fiber-sort partition runs (timing class)
+    int          sort_digit_bits = kDigitBits;  // widest LSD digit of shard sorts / remaps
+    int          fiber_digit_bits = kDigitBits; // widest LSD digit of fiber sorts
     float*       Y[kMaxModes] = {nullptr};
     float*       Yhat[kMaxModes] = {nullptr};
     __nv_bfloat16* Yb[kMaxModes] = {nullptr};
@@ -186,6 +193,7 @@ struct Plan {
     uint32_t*    part_base = nullptr;           // [segments x buckets] bucket starts
     size_t       part_base_cap = 0;
     int*         err_flag = nullptr;            // device-side fault flag
+    uint32_t*    part_ctr = nullptr;            // work-queue counter of the partition scatter
     float*       lambda = nullptr;              // [Rp]
     double*      la_work = nullptr;             // CP-ALS R x R scratch (FP64)
     size_t       la_work_cap = 0;
@@ -207,6 +215,11 @@ struct LaunchTimer {
     ~LaunchTimer();
 };
 int timing_collect(Plan& p);
+
+// Synchronises the plan stream and reads the device fault flag (bounded
+// waits that gave up, out-of-range keys); a raised flag is cleared and
+// reported as DGPU_ERR_DEVICE.
+int sync_checked(Plan& p);
 
 // ---- device memory helpers ----------------------------------------------
 int  dev_alloc(Plan& p, void** ptr, size_t bytes);

@@ -39,12 +39,13 @@
 #include "dgpu_internal.h"
 
 #include <algorithm>
+#include <numeric>
 
 namespace dgpu {
 
 namespace {
 
-constexpr int kHistThreads = 256;
+constexpr int kHistThreads = 1024;
 constexpr int kScatThreads = 512;
 constexpr int kScatWarps = kScatThreads / 32;
 constexpr uint32_t kSegChunkTiles = 16;       // <= 64K elements per segmented chunk
@@ -65,8 +66,19 @@ k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles
     for (uint32_t t = c.tile_begin; t < c.tile_end; ++t) {
         const Tile tl = tiles[t];
         const uint32_t* k = keycol + tl.begin;
-        for (uint32_t j = threadIdx.x; j < tl.count; j += blockDim.x)
-            atomicAdd(&h[part_key(__ldg(k + j), shift, mask)], 1u);
+        // four independent loads in flight per thread
+        const uint32_t rounds = (tl.count + 4 * blockDim.x - 1) / (4 * blockDim.x);
+        for (uint32_t r = 0; r < rounds; ++r) {
+            uint32_t kk[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t j = (r * 4 + q) * blockDim.x + threadIdx.x;
+                kk[q] = j < tl.count ? part_key(__ldg(k + j), shift, mask) : 0xffffffffu;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (kk[q] != 0xffffffffu) atomicAdd(&h[kk[q]], 1u);
+        }
     }
     __syncthreads();
     uint32_t* out = cnt + (size_t)blockIdx.x * nb;
@@ -142,42 +154,164 @@ k_bucket_scan(uint32_t* __restrict__ tot_base, const Seg* __restrict__ segs, uin
     }
 }
 
-// One CTA per chunk.  Window W elements; warp w owns [w*W/16, (w+1)*W/16)
-// of each window; S = W/512 steps of 32 per warp.
+// ---- bulk-copy (TMA) helpers: one elected thread streams each window's
+// columns into shared memory; an mbarrier with a transaction count tells the
+// CTA when they have landed.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait: false after ~2^22 polls (each poll may suspend the thread).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < (1u << 22); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Device fault-flag codes written by the partition kernels.
+constexpr int kErrPartWait = 0x100;      // a bulk copy did not complete in time
+constexpr int kErrPartRange = 0x200;     // a slot outside its window or slab (skipped)
+
+// Next non-empty window of a chunk after (t, w0): windows are W-element
+// pieces of the chunk's tiles in order.  Returns false at the chunk's end.
+template <int W>
+__device__ __forceinline__ bool next_window(const Tile* __restrict__ tiles, uint32_t tend,
+                                            uint32_t& t, uint32_t& w0, Tile& tl)
+{
+    w0 += W;
+    while (w0 >= tl.count) {
+        if (++t >= tend) return false;
+        tl = tiles[t];
+        w0 = 0;
+    }
+    return true;
+}
+
+// Column stride of a window buffer: W elements plus the up-to-3-element head
+// and tail that 16-byte alignment of the bulk copies adds.
+template <int W> constexpr int win_stride() { return W + 8; }
+
+// Streams window (tl.begin + w0, cnt) of every column into `buf` (column c
+// at buf + c * BW); the head (begin & 3) is where element 0 lands.
 template <int N, int W>
-__global__ void __launch_bounds__(kScatThreads, 1)
+__device__ __forceinline__ void issue_window(uint32_t* buf, const SlabPtrs& in, uint32_t src,
+                                             uint32_t cnt, uint64_t* bar)
+{
+    constexpr int BW = win_stride<W>();
+    const uint32_t a = src & ~3u;
+    const uint32_t e = (src + cnt + 3u) & ~3u;
+    const uint32_t bytes = (e - a) * 4u;
+    mbar_expect_tx(bar, bytes * (N + 1));
+    bulk_g2s(buf, in.vals + a, bytes, bar);
+#pragma unroll
+    for (int k = 0; k < N; ++k) bulk_g2s(buf + (size_t)(k + 1) * BW, in.idx[k] + a, bytes, bar);
+}
+
+// Persistent CTAs of 512 threads take chunks from a work queue (largest
+// first).  A chunk is walked in windows of W elements; while window k is
+// ranked and written, window k+1 streams into the other of two shared
+// buffers.  Per window (four block barriers):
+//   a. each warp ranks its W/16 elements (32 per step) with __match_any_sync
+//      and 16-bit per-warp bucket counters;
+//   b. per bucket: exclusive prefix over the 16 warps and the window total;
+//      exclusive scan over buckets; bucket cursors advance by the totals;
+//   c. each element is staged at its bucket-ordered window slot, with its
+//      destination, in the buffer it came from; warps reset their counters;
+//   d. the staged window is written out: consecutive threads store
+//      consecutive slots of one bucket.
+template <int N, int W>
+__global__ void __launch_bounds__(kScatThreads, 2)
 k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
                 const Tile* __restrict__ tiles, const Chunk* __restrict__ chunks,
+                const uint32_t* __restrict__ order, uint32_t nchunks,
                 const uint32_t* __restrict__ off, const uint32_t* __restrict__ base,
-                int key_mode, int shift, uint32_t mask, uint32_t nb)
+                int key_mode, int shift, uint32_t mask, uint32_t nb, uint32_t total,
+                uint32_t* __restrict__ queue, int* __restrict__ err)
 {
     constexpr int S = W / kScatThreads;           // steps per warp per window
     constexpr int PW = W / kScatWarps;            // elements per warp per window
-    extern __shared__ __align__(16) uint32_t sm[];
-    uint32_t* cursor = sm;                                   // [nb]
-    uint32_t* lbase = cursor + nb;                           // [nb]
-    uint16_t* wc = reinterpret_cast<uint16_t*>(lbase + nb);  // [16][nb]
-    uint32_t* stage = lbase + nb + ((size_t)kScatWarps * nb + 1) / 2;
-    float* sv = reinterpret_cast<float*>(stage);             // [W]
-    uint32_t* si = stage + W;                                // [N][W]
-    uint32_t* sd = si + (size_t)N * W;                       // [W]
+    constexpr int BW = win_stride<W>();
+    constexpr int C = N + 2;                      // vals, idx[N], destination
+    constexpr int BPT = kMaxBuckets / kScatThreads;   // buckets per thread, at most
+    extern __shared__ __align__(128) uint32_t sm[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ uint32_t wsum[kScatWarps];
+    __shared__ uint32_t s_chunk[2];     // alternating: a slot is rewritten two barriers later
+    __shared__ int fail;
+    const uint32_t nbp = (nb + 7u) & ~7u;
+    uint32_t* buf = sm;                                      // [2][C][BW]
+    uint32_t* cursor = buf + 2 * C * BW;                     // [nbp]
+    uint32_t* lbase = cursor + nbp;                          // [nbp]
+    uint32_t* dbase = lbase + nbp;                           // [nbp]
+    uint16_t* wc = reinterpret_cast<uint16_t*>(dbase + nbp); // [16][nbp]
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const Chunk c = chunks[blockIdx.x];
-    const uint32_t* o = off + (size_t)blockIdx.x * nb;
-    const uint32_t* bs = base + (size_t)c.seg * nb;
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) cursor[b] = o[b] + bs[b];
-    for (uint32_t i = threadIdx.x; i < kScatWarps * nb; i += blockDim.x) wc[i] = 0;
-    __syncthreads();
+    uint16_t* mywc = wc + (size_t)warp * nbp;
+    for (uint32_t i = threadIdx.x; i < kScatWarps * nbp / 2; i += blockDim.x)
+        reinterpret_cast<uint32_t*>(wc)[i] = 0;
+    if (threadIdx.x == 0) {
+        fail = 0;
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    uint32_t kw = 0;               // windows this CTA has started (mbarrier phases)
+    bool pending = false;          // a bulk copy into buf[kw & 1] is outstanding
 
-    uint16_t* mywc = wc + (size_t)warp * nb;
-    for (uint32_t t = c.tile_begin; t < c.tile_end; ++t) {
-        const Tile tl = tiles[t];
-        for (uint32_t w0 = 0; w0 < tl.count; w0 += W) {
+    for (uint32_t it = 0;; ++it) {
+        if (threadIdx.x == 0) s_chunk[it & 1] = atomicAdd(queue, 1u);
+        __syncthreads();           // previous chunk fully written; s_chunk visible
+        const uint32_t qi = s_chunk[it & 1];
+        if (qi >= nchunks || fail) break;
+        const uint32_t ci = order[qi];
+        const Chunk c = chunks[ci];
+        const uint32_t* o = off + (size_t)ci * nb;
+        const uint32_t* bs = base + (size_t)c.seg * nb;
+        for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) cursor[b] = o[b] + bs[b];
+        // first non-empty window of the chunk
+        if (c.tile_begin >= c.tile_end) continue;
+        uint32_t t = c.tile_begin, w0 = 0u - (uint32_t)W;
+        Tile tl = tiles[t];
+        if (!next_window<W>(tiles, c.tile_end, t, w0, tl)) continue;
+        if (threadIdx.x == 0)
+            issue_window<N, W>(buf + (size_t)(kw & 1) * C * BW, in, tl.begin + w0,
+                               min((uint32_t)W, tl.count - w0), &bar[kw & 1]);
+        pending = true;
+
+        for (;;) {
             const uint32_t cnt = min((uint32_t)W, tl.count - w0);
-            const uint32_t src0 = tl.begin + w0;
-            // a. load + rank
+            const uint32_t head = (tl.begin + w0) & 3u;
+            uint32_t* bk = buf + (size_t)(kw & 1) * C * BW;
+            if (!mbar_wait(&bar[kw & 1], (kw >> 1) & 1u)) {
+                fail = 1;
+                atomicOr(err, kErrPartWait);
+            }
+            // a. load the window's elements and rank them per warp
             uint32_t key[S], rk[S];
             float val[S];
             uint32_t id[S][N];
@@ -185,11 +319,12 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             for (int s = 0; s < S; ++s) {
                 const uint32_t j = warp * PW + s * 32 + lane;
                 const bool act = j < cnt;
-                const uint32_t src = src0 + (act ? j : 0);
-                key[s] = act ? part_key(__ldg(in.idx[key_mode] + src), shift, mask) : 0xffffffffu;
-                val[s] = __ldg(in.vals + src);
+                const uint32_t q = head + (act ? j : 0);
 #pragma unroll
-                for (int k = 0; k < N; ++k) id[s][k] = __ldg(in.idx[k] + src);
+                for (int m = 0; m < N; ++m) id[s][m] = bk[(size_t)(m + 1) * BW + q];
+                val[s] = __uint_as_float(bk[q]);
+                const uint32_t kv = bk[(size_t)(key_mode + 1) * BW + q];
+                key[s] = act ? part_key(kv, shift, mask) : 0xffffffffu;
             }
 #pragma unroll
             for (int s = 0; s < S; ++s) {
@@ -205,90 +340,108 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                 }
                 __syncwarp();
             }
-            __syncthreads();
-            // b. per-bucket warp prefixes and window bucket totals -> lbase
-            for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
-                uint32_t run = 0;
+            __syncthreads();       // (1) buffer read, counters complete, `fail` visible
+            if (fail) break;
+            pending = false;
+            // prefetch the next window into the other buffer: its last reader
+            // (window kw-1's write-out) finished before barrier (1)
+            uint32_t nt = t, nw0 = w0;
+            Tile ntl = tl;
+            const bool more = next_window<W>(tiles, c.tile_end, nt, nw0, ntl);
+            if (more && threadIdx.x == 0)
+                issue_window<N, W>(buf + (size_t)((kw + 1) & 1) * C * BW, in, ntl.begin + nw0,
+                                   min((uint32_t)W, ntl.count - nw0), &bar[(kw + 1) & 1]);
+            // b. warp prefixes per bucket (only counters a warp used become
+            //    prefixes, so the warps' resets in c leave all counters zero)
+            const uint32_t per = (nb + kScatThreads - 1) / kScatThreads;
+            const uint32_t b0 = threadIdx.x * per;
+            uint32_t tot[BPT];
+            uint32_t sum = 0;
 #pragma unroll
-                for (int w = 0; w < kScatWarps; ++w) {
-                    const uint32_t v = wc[(size_t)w * nb + b];
-                    wc[(size_t)w * nb + b] = (uint16_t)run;
-                    run += v;
+            for (int u = 0; u < BPT; ++u) {
+                tot[u] = 0;
+                const uint32_t b = b0 + u;
+                if ((uint32_t)u < per && b < nb) {
+                    uint32_t run = 0;
+#pragma unroll
+                    for (int w = 0; w < kScatWarps; ++w) {
+                        const uint32_t v = wc[(size_t)w * nbp + b];
+                        if (v) wc[(size_t)w * nbp + b] = (uint16_t)run;
+                        run += v;
+                    }
+                    tot[u] = run;
+                    sum += run;
                 }
-                lbase[b] = run;
             }
-            __syncthreads();
-            // exclusive scan of lbase over buckets (each thread a run of buckets)
+            uint32_t x = sum;
+#pragma unroll
+            for (int q = 1; q < 32; q <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, q);
+                if (lane >= q) x += y;
+            }
+            if (lane == 31) wsum[warp] = x;
+            __syncthreads();       // (2)
             {
-                __shared__ uint32_t wsum[kScatWarps];
-                const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-                const uint32_t b0 = threadIdx.x * per;
-                uint32_t s = 0;
-                for (uint32_t k = 0; k < per; ++k)
-                    if (b0 + k < nb) s += lbase[b0 + k];
-                uint32_t x = s;
+                uint32_t v = (lane < warp) ? wsum[lane] : 0u;
 #pragma unroll
-                for (int q = 1; q < 32; q <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, q);
-                    if (lane >= q) x += y;
-                }
-                if (lane == 31) wsum[warp] = x;
-                __syncthreads();
-                if (warp == 0) {
-                    uint32_t v = lane < kScatWarps ? wsum[lane] : 0u;
+                for (int q = 16; q >= 1; q >>= 1) v += __shfl_xor_sync(0xffffffffu, v, q);
+                uint32_t pre = v + x - sum;
 #pragma unroll
-                    for (int q = 1; q < 32; q <<= 1) {
-                        const uint32_t y = __shfl_up_sync(0xffffffffu, v, q);
-                        if (lane >= q) v += y;
+                for (int u = 0; u < BPT; ++u) {
+                    const uint32_t b = b0 + u;
+                    if ((uint32_t)u < per && b < nb) {
+                        const uint32_t cur = cursor[b];
+                        lbase[b] = pre;
+                        dbase[b] = cur - pre;
+                        cursor[b] = cur + tot[u];
+                        pre += tot[u];
                     }
-                    if (lane < kScatWarps) wsum[lane] = v;
                 }
-                __syncthreads();
-                uint32_t pre = (warp ? wsum[warp - 1] : 0u) + x - s;
-                for (uint32_t k = 0; k < per; ++k)
-                    if (b0 + k < nb) {
-                        const uint32_t v = lbase[b0 + k];
-                        lbase[b0 + k] = pre;
-                        pre += v;
-                    }
             }
-            __syncthreads();
-            // c. stage in bucket order with the global slot of each element
+            __syncthreads();       // (3)
+            // c. stage in bucket order with each element's destination
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
-                const uint32_t within = (uint32_t)mywc[key[s]] + rk[s];
-                const uint32_t lp = lbase[key[s]] + within;
-                sv[lp] = val[s];
+                const uint32_t lp = lbase[key[s]] + mywc[key[s]] + rk[s];
+                if (lp >= cnt) { atomicOr(err, kErrPartRange); continue; }
+                bk[lp] = __float_as_uint(val[s]);
 #pragma unroll
-                for (int k = 0; k < N; ++k) si[(size_t)k * W + lp] = id[s][k];
-                sd[lp] = cursor[key[s]] + within;
+                for (int m = 0; m < N; ++m) bk[(size_t)(m + 1) * BW + lp] = id[s][m];
+                bk[(size_t)(N + 1) * BW + lp] = dbase[key[s]] + lp;
             }
-            __syncthreads();
-            // d. coalesced write-out, runs of one bucket are contiguous
-            for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-                const uint32_t d = sd[i];
-                out.vals[d] = sv[i];
+            __syncwarp();
 #pragma unroll
-                for (int k = 0; k < N; ++k) out.idx[k][d] = si[(size_t)k * W + i];
+            for (int s = 0; s < S; ++s)
+                if (key[s] != 0xffffffffu) mywc[key[s]] = 0;
+            __syncthreads();       // (4)
+            // d. write-out: runs of one bucket are contiguous
+            for (uint32_t i = threadIdx.x; i < cnt; i += kScatThreads) {
+                const uint32_t d = bk[(size_t)(N + 1) * BW + i];
+                if (d >= total) { atomicOr(err, kErrPartRange); continue; }
+                out.vals[d] = __uint_as_float(bk[i]);
+#pragma unroll
+                for (int m = 0; m < N; ++m) out.idx[m][d] = bk[(size_t)(m + 1) * BW + i];
             }
-            // e. advance the cursors, clear the warp counters
-            for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
-                const uint32_t next = (b + 1 < nb) ? lbase[b + 1] : cnt;
-                cursor[b] += next - lbase[b];
-            }
-            for (uint32_t i = threadIdx.x; i < kScatWarps * nb; i += blockDim.x) wc[i] = 0;
-            __syncthreads();
+            fence_proxy_async_smem();   // generic accesses before a later bulk write
+            ++kw;
+            if (!more) break;
+            pending = true;
+            t = nt; w0 = nw0; tl = ntl;
         }
+        if (fail) break;
     }
+    // leave no bulk copy in flight into this CTA's shared memory
+    if (fail && pending && threadIdx.x == 0) mbar_wait(&bar[kw & 1], (kw >> 1) & 1u);
 }
 
 template <int N>
-constexpr int scatter_window() { return N <= 4 ? 4096 : 2048; }
+constexpr int scatter_window() { return N <= 4 ? 2048 : 1024; }
 
 size_t scatter_smem(int N, uint32_t nb) {
-    const int W = N <= 4 ? 4096 : 2048;
-    return ((size_t)2 * nb + ((size_t)kScatWarps * nb + 1) / 2 + (size_t)(2 + N) * W) * 4;
+    const size_t W = N <= 4 ? 2048 : 1024;
+    const size_t nbp = (nb + 7u) & ~7u;
+    return (2 * (size_t)(N + 2) * (W + 8) + 3 * nbp) * 4 + (size_t)kScatWarps * nbp * 2;
 }
 
 int ensure_part_scratch(Plan& p, size_t entries, size_t base_entries) {
@@ -317,16 +470,22 @@ int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, 
 {
     constexpr int W = scatter_window<N>();
     const size_t smem = scatter_smem(N, nb);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static uint64_t attr_set = 0;          // per device (function attributes are per context)
+    const uint64_t dbit = 1ull << (p.device & 63);
+    if (!(attr_set & dbit)) {
         DGPU_CUDA(cudaFuncSetAttribute(k_chunk_scatter<N, W>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)scatter_smem(N, kMaxBuckets)));
-        attr_set = true;
+        attr_set |= dbit;
     }
-    k_chunk_scatter<N, W><<<L.nchunks, kScatThreads, smem, p.stream>>>(
-        slab_in(in, p.N), slab_out(out, p.N), L.tiles, L.chunks, p.part_off, p.part_base,
-        key_mode, key_shift, key_mask, nb);
+    int per_sm = 0;
+    DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chunk_scatter<N, W>,
+                                                            kScatThreads, smem));
+    const uint32_t grid = std::max(1u, std::min(L.nchunks, (uint32_t)(std::max(1, per_sm) * p.sms)));
+    DGPU_CUDA(cudaMemsetAsync(p.part_ctr, 0, sizeof(uint32_t), p.stream));
+    k_chunk_scatter<N, W><<<grid, kScatThreads, smem, p.stream>>>(
+        slab_in(in, p.N), slab_out(out, p.N), L.tiles, L.chunks, L.order, L.nchunks, p.part_off,
+        p.part_base, key_mode, key_shift, key_mask, nb, (uint32_t)p.nnz, p.part_ctr, p.err_flag);
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
 }
@@ -337,6 +496,7 @@ void free_partlist(PartList& l) {
     if (l.own_tiles) dev_free(l.tiles);
     dev_free(l.chunks);
     dev_free(l.segs);
+    dev_free(l.order);
     l = PartList{};
 }
 
@@ -348,19 +508,22 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     std::vector<Chunk> ch;
     std::vector<Seg> sg;
     if (global) {
-        // ~2 chunks per SM of roughly equal element counts
+        // 4 chunks per SM of near-equal element counts (cut where the running
+        // total crosses the next multiple of total / want), so the chunk
+        // count divides evenly over 1 or 2 resident scatter CTAs per SM
         uint64_t total = 0;
         for (const Tile& t : tiles) total += t.count;
-        const uint64_t target = std::max<uint64_t>(kTile, (total + 2 * p.sms - 1) / (2 * p.sms));
+        const uint64_t want = std::max<uint64_t>(
+            1, std::min<uint64_t>(4ull * (uint64_t)p.sms, (total + kTile - 1) / kTile));
         Seg s{0, 0, 0, 0};
         uint32_t t0 = 0;
         uint64_t acc = 0;
         for (uint32_t t = 0; t < tiles.size(); ++t) {
             acc += tiles[t].count;
-            if (acc >= target || t + 1 == tiles.size()) {
+            const uint64_t cut = (ch.size() + 1) * total / want;
+            if (acc >= cut || t + 1 == tiles.size()) {
                 ch.push_back(Chunk{t0, t + 1, 0, 0});
                 t0 = t + 1;
-                acc = 0;
             }
         }
         s.chunk_end = (uint32_t)ch.size();
@@ -380,6 +543,14 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
             sg[s].chunk_end = (uint32_t)ch.size();
         }
     }
+    // work order of the persistent scatter: largest chunks first
+    std::vector<uint64_t> csize(ch.size(), 0);
+    for (size_t c = 0; c < ch.size(); ++c)
+        for (uint32_t t = ch[c].tile_begin; t < ch[c].tile_end; ++t) csize[c] += tiles[t].count;
+    std::vector<uint32_t> order(ch.size());
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return csize[a] > csize[b]; });
     out.ntiles = (uint32_t)tiles.size();
     out.nchunks = (uint32_t)ch.size();
     out.nsegs = (uint32_t)sg.size();
@@ -395,9 +566,13 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     }
     DGPU_TRY(dev_alloc(p, (void**)&out.chunks, std::max<size_t>(1, ch.size()) * sizeof(Chunk)));
     DGPU_TRY(dev_alloc(p, (void**)&out.segs, std::max<size_t>(1, sg.size()) * sizeof(Seg)));
-    if (!ch.empty())
+    DGPU_TRY(dev_alloc(p, (void**)&out.order, std::max<size_t>(1, ch.size()) * sizeof(uint32_t)));
+    if (!ch.empty()) {
         DGPU_CUDA(cudaMemcpyAsync(out.chunks, ch.data(), ch.size() * sizeof(Chunk),
                                   cudaMemcpyHostToDevice, p.stream));
+        DGPU_CUDA(cudaMemcpyAsync(out.order, order.data(), order.size() * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice, p.stream));
+    }
     DGPU_CUDA(cudaMemcpyAsync(out.segs, sg.data(), sg.size() * sizeof(Seg), cudaMemcpyHostToDevice,
                               p.stream));
     DGPU_CUDA(cudaStreamSynchronize(p.stream));
@@ -416,19 +591,21 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
     const double elem = (double)p.nnz;
     const double row_bytes = 4.0 + 4.0 * p.N;
     {
-        LaunchTimer t(p, KK_PART_HIST, elem * 4.0 + (double)L.nchunks * nb * 4.0);
+        LaunchTimer t(p, p.part_fiber ? KK_FIB_HIST : KK_PART_HIST,
+                      elem * 4.0 + (double)L.nchunks * nb * 4.0);
         k_chunk_hist<<<L.nchunks, kHistThreads, nb * sizeof(uint32_t), p.stream>>>(
             in.idx[key_mode], L.tiles, L.chunks, key_shift, key_mask, nb, p.part_cnt);
         DGPU_CUDA(cudaGetLastError());
     }
     {
-        LaunchTimer t(p, KK_PART_SCAN, (double)L.nchunks * nb * 8.0);
+        LaunchTimer t(p, p.part_fiber ? KK_FIB_SCAN : KK_PART_SCAN, (double)L.nchunks * nb * 8.0);
         dim3 g(L.nsegs, (nb + 255) / 256);
         k_col_scan<<<g, 256, 0, p.stream>>>(p.part_cnt, L.segs, nb, p.part_off, p.part_base);
         k_bucket_scan<<<L.nsegs, 1024, 0, p.stream>>>(p.part_base, L.segs, nb);
         DGPU_CUDA(cudaGetLastError());
     }
-    LaunchTimer t(p, KK_PART_SCATTER, elem * 2.0 * row_bytes + (double)L.nchunks * nb * 4.0);
+    LaunchTimer t(p, p.part_fiber ? KK_FIB_SCATTER : KK_PART_SCATTER,
+                  elem * 2.0 * row_bytes + (double)L.nchunks * nb * 4.0);
     switch (p.N) {
 #define DGPU_SC(NN) case NN: return launch_scatter<NN>(p, in, out, L, key_mode, key_shift, key_mask, nb)
         DGPU_SC(2); DGPU_SC(3); DGPU_SC(4); DGPU_SC(5); DGPU_SC(6); DGPU_SC(7); DGPU_SC(8);
@@ -445,7 +622,8 @@ int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first, int key_m
     int bits = 0;
     while (bits < 32 && ((uint64_t)1 << bits) < key_limit) ++bits;
     if (key_limit <= 1) bits = 1;
-    int passes = (bits + kDigitBits - 1) / kDigitBits;
+    const int digit = std::max(1, std::min(kDigitBits, p.sort_digit_bits));
+    int passes = (bits + digit - 1) / digit;
     if (passes < 1) passes = 1;
     const int dbits = (bits + passes - 1) / passes;
     int src = a, dst = b;
@@ -478,16 +656,20 @@ int fiber_sort(Plan& p, int n, int src, int other, int* result) {
         set_error("fiber_sort: mode %d has no fiber tile list", n);
         return DGPU_ERR_NOT_BUILT;
     }
-    const int passes = (bits + kDigitBits - 1) / kDigitBits;
+    const int digit = std::max(1, std::min(kDigitBits, p.fiber_digit_bits));
+    const int passes = (bits + digit - 1) / digit;
     const int dbits = (bits + passes - 1) / passes;
     int a = src, b = other;
+    p.part_fiber = 1;
     for (int k = 0; k < passes; ++k) {
         const int sh = k * dbits;
         const int hi = std::min(bits, sh + dbits);
         const uint32_t mask = (1u << (hi - sh)) - 1u;
-        DGPU_TRY(stable_partition(p, p.slab[a], p.fib[n], n, sh, mask, mask + 1, p.slab[b]));
+        const int rc = stable_partition(p, p.slab[a], p.fib[n], n, sh, mask, mask + 1, p.slab[b]);
+        if (rc != DGPU_OK) { p.part_fiber = 0; return rc; }
         std::swap(a, b);
     }
+    p.part_fiber = 0;
     *result = a;
     return DGPU_OK;
 }

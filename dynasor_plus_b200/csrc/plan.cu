@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <queue>
@@ -75,6 +76,23 @@ int slab_alloc(Plan& p, Slab& s) {
     for (int n = 0; n < p.N; ++n) {
         s.idx[n] = reinterpret_cast<uint32_t*>(c);
         c += ib;
+    }
+    return DGPU_OK;
+}
+
+int sync_checked(Plan& p) {
+    int flag = 0;
+    if (p.err_flag)
+        DGPU_CUDA(cudaMemcpyAsync(&flag, p.err_flag, sizeof(int), cudaMemcpyDeviceToHost, p.stream));
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    if (flag) {
+        DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
+        DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        set_error("device fault flag 0x%x: %s", flag,
+                  (flag & 0x100) ? "a partition kernel's bulk copy did not complete in time"
+                  : (flag & 0x200) ? "a partition kernel computed an out-of-range slot"
+                                   : "a device-side check failed");
+        return DGPU_ERR_DEVICE;
     }
     return DGPU_OK;
 }
@@ -159,6 +177,7 @@ Plan::~Plan() {
     dev_free(part_off);
     dev_free(part_base);
     dev_free(err_flag);
+    dev_free(part_ctr);
     dev_free(lambda);
     dev_free(la_work);
     dev_free(la_f32);
@@ -320,6 +339,10 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
         p.own_stream = true;
     }
     DGPU_CUDA(cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, p.device));
+    // digit widths of the LSD partition passes (tuning knobs; the permutation
+    // does not depend on them)
+    if (const char* e = std::getenv("DGPU_SORT_DIGIT_BITS")) p.sort_digit_bits = std::atoi(e);
+    if (const char* e = std::getenv("DGPU_FIBER_DIGIT_BITS")) p.fiber_digit_bits = std::atoi(e);
 
     // geometry
     for (int n = 0; n < p.N; ++n) {
@@ -345,6 +368,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     for (int s = 0; s < nslab; ++s) DGPU_TRY(slab_alloc(p, p.slab[s]));
     DGPU_TRY(dev_alloc(p, (void**)&p.err_flag, sizeof(int)));
     DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
+    DGPU_TRY(dev_alloc(p, (void**)&p.part_ctr, sizeof(uint32_t)));
 
     // input COO -> slab[1] (the reference's loader order)
     const int in_slab = 1;
@@ -470,7 +494,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
         p.yb_stale[n] = true;
     }
     DGPU_TRY(dev_alloc(p, (void**)&p.lambda, (size_t)p.Rp * sizeof(float)));
-    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    DGPU_TRY(sync_checked(p));
     return DGPU_OK;
 }
 
