@@ -51,10 +51,12 @@ METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--threads", type=int, default=8, help="plan worker count (FLYCOO geometry)")
+    ap.add_argument("--threads", type=int, default=16,
+                    help="plan worker count: the FLYCOO geometry of the reference run with "
+                         "this many threads (16 = the GPU host's cores)")
     ap.add_argument("--layout", default="pingpong", choices=["pingpong", "ncopy"])
     ap.add_argument("--fiber", type=int, default=1)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])

@@ -34,6 +34,7 @@ constexpr uint32_t kTile = 4096;
 // into least-significant-digit passes of this many buckets.
 constexpr uint32_t kMaxBuckets = 2048;
 constexpr int kDigitBits = 11;   // log2(kMaxBuckets)
+constexpr int kDefaultDigitBits = 8;
 
 // ----------------------------------------------------------------------------
 //  Error plumbing (thread-local last error, status codes, no exit()).
@@ -181,8 +182,12 @@ struct Plan {
     PartList     ident;                         // identity order over [0, nnz) (global)
     int          sms = 148;                     // SM count of the device
     int          part_fiber = 0;                // 1 while a fiber-sort partition runs (timing class)
-    int          sort_digit_bits = kDigitBits;  // widest LSD digit of shard sorts / remaps
-    int          fiber_digit_bits = kDigitBits; // widest LSD digit of fiber sorts
+    // Widest LSD digit of shard sorts / remaps and of fiber sorts.  Above ~8
+    // bits a pass writes runs of a few elements per bucket and window, which
+    // costs more (uncoalesced stores, partial-sector DRAM writes) than a
+    // second pass with narrow digits.
+    int          sort_digit_bits = kDefaultDigitBits;
+    int          fiber_digit_bits = kDefaultDigitBits;
     float*       Y[kMaxModes] = {nullptr};
     float*       Yhat[kMaxModes] = {nullptr};
     __nv_bfloat16* Yb[kMaxModes] = {nullptr};

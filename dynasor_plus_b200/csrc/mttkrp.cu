@@ -92,10 +92,15 @@ __device__ __forceinline__ float gather1(const FacPtrs& F, int w, uint32_t row, 
 constexpr int kRunThreads = 256;
 constexpr int kRunWarps = kRunThreads / 32;
 
-template <int N, int V>
+// Nonzeros whose gathers a lane group keeps in flight together (U) and the
+// CTAs per SM the kernel is compiled for.  The kernel is bound by gather
+// latency, so occupancy (64 registers, 4 CTAs of 256 threads) pays more than
+// a deeper batch; BF16 rows take half the registers, so BF16 batches deeper.
+template <int N, int V, bool BF>
 struct RunBatch {
     static constexpr int kWork = (N - 1) * V;
-    static constexpr int U = kWork <= 2 ? 4 : (kWork <= 4 ? 2 : 1);
+    static constexpr int U = kWork <= 2 ? (BF ? 4 : 2) : (kWork <= 4 ? 2 : 1);
+    static constexpr int kMinBlocks = N <= 4 ? 4 : 2;
 };
 
 // One CTA per tile.  Warp w owns the w-th contiguous slice of the tile and
@@ -109,7 +114,7 @@ struct RunBatch {
 // specialisation, src/dynasor_kernel.cpp:247-265), so only the N-1 gathered
 // rows occupy registers; TN = -1 takes the mode at run time.
 template <int N, int G, int V, bool BF, int TN>
-__global__ void __launch_bounds__(kRunThreads, 2)
+__global__ void __launch_bounds__(kRunThreads, (RunBatch<N, V, BF>::kMinBlocks))
 k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ tiles,
                 const __grid_constant__ FacPtrs F, float* __restrict__ Yhat,
                 int n_rt, int w0_rt, int wl_rt, int Rp)
@@ -117,7 +122,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     const int n = TN >= 0 ? TN : n_rt;
     const int w0 = TN >= 0 ? (TN == 0 ? 1 : 0) : w0_rt;
     const int wl = TN >= 0 ? (N == 2 ? -1 : (TN == N - 1 ? N - 2 : N - 1)) : wl_rt;
-    constexpr int U = RunBatch<N, V>::U;
+    constexpr int U = RunBatch<N, V, BF>::U;
     constexpr int NG = 32 / G;                    // groups per warp
     constexpr int CH = G >= 16 ? G : ((1 + N + 3) / 4 * 4 > 8 ? 8 : 16);  // staged per group
     constexpr int LPE = CH / G;                   // nonzeros loaded per lane per chunk

@@ -231,6 +231,14 @@ __device__ __forceinline__ void issue_window(uint32_t* buf, const SlabPtrs& in, 
     for (int k = 0; k < N; ++k) bulk_g2s(buf + (size_t)(k + 1) * BW, in.idx[k] + a, bytes, bar);
 }
 
+// Window size of the scatter and its buffer column count: N+1 input
+// columns; staging needs a 16-byte record + destination (5 words) when
+// N <= 3, else N+2 columns.
+template <int N>
+constexpr int scatter_window() { return N <= 4 ? 2048 : 1024; }
+template <int N>
+constexpr int scatter_cols() { return N + 1 <= 4 ? 5 : N + 2; }
+
 // Persistent CTAs of 512 threads take chunks from a work queue (largest
 // first).  A chunk is walked in windows of W elements; while window k is
 // ranked and written, window k+1 streams into the other of two shared
@@ -255,7 +263,10 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     constexpr int S = W / kScatThreads;           // steps per warp per window
     constexpr int PW = W / kScatWarps;            // elements per warp per window
     constexpr int BW = win_stride<W>();
-    constexpr int C = N + 2;                      // vals, idx[N], destination
+    // staged element: one 16-byte record (val, idx...) when N <= 3, else columns
+    constexpr bool kRec = (N + 1 <= 4);
+    constexpr int C = scatter_cols<N>();          // buffer columns (input, then stage)
+    constexpr int DC = kRec ? 4 : N + 1;          // column holding staged destinations
     constexpr int BPT = kMaxBuckets / kScatThreads;   // buckets per thread, at most
     extern __shared__ __align__(128) uint32_t sm[];
     __shared__ __align__(8) uint64_t bar[2];
@@ -265,9 +276,8 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     const uint32_t nbp = (nb + 7u) & ~7u;
     uint32_t* buf = sm;                                      // [2][C][BW]
     uint32_t* cursor = buf + 2 * C * BW;                     // [nbp]
-    uint32_t* lbase = cursor + nbp;                          // [nbp]
-    uint32_t* dbase = lbase + nbp;                           // [nbp]
-    uint16_t* wc = reinterpret_cast<uint16_t*>(dbase + nbp); // [16][nbp]
+    uint2* ld = reinterpret_cast<uint2*>(cursor + nbp);      // [nbp] {window base, dest - slot}
+    uint16_t* wc = reinterpret_cast<uint16_t*>(ld + nbp);    // [16][nbp]
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -391,8 +401,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                     const uint32_t b = b0 + u;
                     if ((uint32_t)u < per && b < nb) {
                         const uint32_t cur = cursor[b];
-                        lbase[b] = pre;
-                        dbase[b] = cur - pre;
+                        ld[b] = make_uint2(pre, cur - pre);
                         cursor[b] = cur + tot[u];
                         pre += tot[u];
                     }
@@ -403,12 +412,20 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
-                const uint32_t lp = lbase[key[s]] + mywc[key[s]] + rk[s];
+                const uint2 bd = ld[key[s]];
+                const uint32_t lp = bd.x + mywc[key[s]] + rk[s];
                 if (lp >= cnt) { atomicOr(err, kErrPartRange); continue; }
-                bk[lp] = __float_as_uint(val[s]);
+                if constexpr (kRec) {
+                    uint32_t r[4] = {__float_as_uint(val[s]), 0u, 0u, 0u};
 #pragma unroll
-                for (int m = 0; m < N; ++m) bk[(size_t)(m + 1) * BW + lp] = id[s][m];
-                bk[(size_t)(N + 1) * BW + lp] = dbase[key[s]] + lp;
+                    for (int m = 0; m < N; ++m) r[m + 1] = id[s][m];
+                    reinterpret_cast<uint4*>(bk)[lp] = make_uint4(r[0], r[1], r[2], r[3]);
+                } else {
+                    bk[lp] = __float_as_uint(val[s]);
+#pragma unroll
+                    for (int m = 0; m < N; ++m) bk[(size_t)(m + 1) * BW + lp] = id[s][m];
+                }
+                bk[(size_t)DC * BW + lp] = bd.y + lp;
             }
             __syncwarp();
 #pragma unroll
@@ -417,11 +434,19 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             __syncthreads();       // (4)
             // d. write-out: runs of one bucket are contiguous
             for (uint32_t i = threadIdx.x; i < cnt; i += kScatThreads) {
-                const uint32_t d = bk[(size_t)(N + 1) * BW + i];
+                const uint32_t d = bk[(size_t)DC * BW + i];
                 if (d >= total) { atomicOr(err, kErrPartRange); continue; }
-                out.vals[d] = __uint_as_float(bk[i]);
+                if constexpr (kRec) {
+                    const uint4 r = reinterpret_cast<const uint4*>(bk)[i];
+                    const uint32_t rv[4] = {r.x, r.y, r.z, r.w};
+                    out.vals[d] = __uint_as_float(rv[0]);
 #pragma unroll
-                for (int m = 0; m < N; ++m) out.idx[m][d] = bk[(size_t)(m + 1) * BW + i];
+                    for (int m = 0; m < N; ++m) out.idx[m][d] = rv[m + 1];
+                } else {
+                    out.vals[d] = __uint_as_float(bk[i]);
+#pragma unroll
+                    for (int m = 0; m < N; ++m) out.idx[m][d] = bk[(size_t)(m + 1) * BW + i];
+                }
             }
             fence_proxy_async_smem();   // generic accesses before a later bulk write
             ++kw;
@@ -435,13 +460,13 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     if (fail && pending && threadIdx.x == 0) mbar_wait(&bar[kw & 1], (kw >> 1) & 1u);
 }
 
-template <int N>
-constexpr int scatter_window() { return N <= 4 ? 2048 : 1024; }
 
-size_t scatter_smem(int N, uint32_t nb) {
-    const size_t W = N <= 4 ? 2048 : 1024;
+
+template <int N>
+size_t scatter_smem(uint32_t nb) {
     const size_t nbp = (nb + 7u) & ~7u;
-    return (2 * (size_t)(N + 2) * (W + 8) + 3 * nbp) * 4 + (size_t)kScatWarps * nbp * 2;
+    return (2 * (size_t)scatter_cols<N>() * win_stride<scatter_window<N>()>() + 3 * nbp) * 4 +
+           (size_t)kScatWarps * nbp * 2;
 }
 
 int ensure_part_scratch(Plan& p, size_t entries, size_t base_entries) {
@@ -469,13 +494,13 @@ int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, 
                    int key_shift, uint32_t key_mask, uint32_t nb)
 {
     constexpr int W = scatter_window<N>();
-    const size_t smem = scatter_smem(N, nb);
+    const size_t smem = scatter_smem<N>(nb);
     static uint64_t attr_set = 0;          // per device (function attributes are per context)
     const uint64_t dbit = 1ull << (p.device & 63);
     if (!(attr_set & dbit)) {
         DGPU_CUDA(cudaFuncSetAttribute(k_chunk_scatter<N, W>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)scatter_smem(N, kMaxBuckets)));
+                                       (int)scatter_smem<N>(kMaxBuckets)));
         attr_set |= dbit;
     }
     int per_sm = 0;
