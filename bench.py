@@ -47,6 +47,17 @@ SEED = 2
 RANK = 32
 METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per nonzero per
+# launch, from one ncu capture of the same kernels on the 20M-draw case of
+# this workload (14,569,916 nnz; profiles/traffic_zipf1.1_14.6M.md).  Both
+# kernels stream the slab once per launch, so their traffic grows with nnz;
+# the bench scales these figures to its own nnz for `roofline.traffic`.
+NCU_DRAM_BYTES_PER_NNZ = {
+    "part_scatter": 29.49,     # k_chunk_scatter, all launches averaged
+    "fiber_scatter": 29.49,
+    "mttkrp": 35.36,           # k_mttkrp_rowrun, 3 modes averaged
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -354,9 +365,17 @@ def main():
                            "peak_gbs": peak, "frac": algo / (ms_step * 1e-3) / 1e9 / peak,
                            "peak_source": peak_src},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (NCU_DRAM_BYTES_PER_NNZ[dom] * nnz
+                                 if dom in NCU_DRAM_BYTES_PER_NNZ else None),
+                     "traffic_source": "ncu dram bytes per nnz on the 14.6M-nnz case, scaled",
                      "peak_source": peak_src, "avg_launch_ms": dom_ms,
                      "algorithmic_bytes_per_launch": dom_bytes},
+        "kernel_rooflines": {
+            k: {"achieved_gbs": (v["bytes"] / v["launches"]) / (v["total_ms"] / v["launches"] * 1e-3) / 1e9,
+                "frac": (v["bytes"] / v["launches"]) / (v["total_ms"] / v["launches"] * 1e-3) / 1e9 / peak,
+                "avg_launch_ms": v["total_ms"] / v["launches"]}
+            for k, v in tim.items() if v["launches"] and v["total_ms"] > 0},
         "kernel_times_ms_per_step": {k: v["total_ms"] / 2 for k, v in tim.items() if v["launches"]},
         "kernel_share": {k: v["total_ms"] / total_ms for k, v in tim.items() if v["launches"]},
         "gpu_launches": launches_per_step * args.steps,
