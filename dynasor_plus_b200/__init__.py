@@ -238,7 +238,7 @@ class Plan:
 
     # -- CP-ALS / CP-OPT -------------------------------------------------------------
     def cpals(self, max_iters=50, tol=1e-4, seed=42, ridge=1e-10, kernel="gs",
-              solve_fp64=True, use_init=False, verbose=False):
+              solve_fp64=True, use_init=False, verbose=False, graphs=True):
         o = CpOptions()
         lib().dgpu_cp_options_default(C.byref(o))
         o.max_iters = int(max_iters)
@@ -249,6 +249,7 @@ class Plan:
         o.solve_fp64 = 1 if solve_fp64 else 0
         o.use_init = 1 if use_init else 0
         o.verbose = 1 if verbose else 0
+        o.graphs = 1 if graphs else 0
         r = CpResult()
         hist = np.zeros(max(1, int(max_iters)), np.float64)
         check(lib().dgpu_cpals(self._h, C.byref(o), C.byref(r), hist.ctypes.data))

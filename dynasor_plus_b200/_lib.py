@@ -50,7 +50,7 @@ class PlanInfo(C.Structure):
 class CpOptions(C.Structure):
     _fields_ = [("max_iters", C.c_int), ("tol", C.c_double), ("seed", C.c_uint64),
                 ("ridge", C.c_double), ("kernel", C.c_int), ("solve_fp64", C.c_int),
-                ("use_init", C.c_int), ("verbose", C.c_int)]
+                ("use_init", C.c_int), ("verbose", C.c_int), ("graphs", C.c_int)]
 
 
 class CpResult(C.Structure):

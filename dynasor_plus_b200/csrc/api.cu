@@ -373,6 +373,7 @@ void dgpu_cp_options_default(dgpu_cp_options* o) {
     o->solve_fp64 = 1;
     o->use_init = 0;
     o->verbose = 0;
+    o->graphs = 1;
 }
 
 int dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt, dgpu_cp_result* res,

@@ -292,6 +292,227 @@ k_fit(const double* __restrict__ Gd, int N, int R, const double* __restrict__ la
     }
 }
 
+// The whole factor update of a small mode in one CTA (rows * Rp <= 8192,
+// R <= 64; the new factor is built in shared memory): Hadamard of the other Grams + relative ridge, Cholesky, the
+// solve map W, Y = Yhat W, the Gram of Y, lambda from its diagonal, the
+// normalised Gram, column scaling and, for the last mode, the fit.  The same
+// arithmetic as the multi-kernel path (k_build_solve_map, k_apply_map,
+// k_gram_partial, k_finalize_mode, k_scale_cols, k_fit) except that the
+// Gram is summed in FP64 throughout; one launch instead of six keeps small
+// tensors from being bound by launch latency.
+template <typename Real>
+__global__ void __launch_bounds__(1024)
+k_update_small(double* __restrict__ Gd, float* __restrict__ G32, int N, int n, int R, int Rp,
+               double ridge, const float* __restrict__ Yhat, float* __restrict__ Y, uint32_t rows,
+               float* __restrict__ lambda, double* __restrict__ lam64, int last, double tnorm2,
+               double* __restrict__ fitout)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int RR = R * R;
+    double* Wx = reinterpret_cast<double*>(smraw);         // R x R solve map (FP64)
+    double* G = Wx + RR;                                    // R x R Gram
+    double* lam = G + RR;                                   // R
+    double* dot = lam + R;                                  // R
+    const int LDA = R + 1;                                  // padded: lanes own rows
+    Real* A = reinterpret_cast<Real*>(dot + R);             // R x LDA Cholesky work
+    Real* invd = A + R * LDA;                               // R: 1 / pivot (0 for a zero pivot)
+    float* Ys = reinterpret_cast<float*>(invd + R);         // rows x Rp: the new factor
+    float* Hs = Ys + (size_t)rows * Rp;                     // rows x Rp: Yhat
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t total = rows * (uint32_t)Rp;
+    for (uint32_t e = tid; e < total; e += nt) Hs[e] = __ldg(Yhat + e);
+
+    for (int e = tid; e < RR; e += nt) {
+        double v = 1.0;
+        for (int m = 0; m < N; ++m)
+            if (m != n) v *= Gd[(size_t)m * RR + e];
+        A[(e / R) * LDA + e % R] = (Real)v;
+        G[e] = 0.0;
+    }
+    for (int r = tid; r < R; r += nt) dot[r] = 0.0;
+    __syncthreads();
+    // Ridge, Cholesky and the solve map run in warp 0 alone (warp barriers
+    // only); the other warps wait at the next block barrier.
+    if (tid < 32) {
+        const int lane = tid;
+        Real dmax = 0;
+        for (int r = lane; r < R; r += 32) dmax = max(dmax, A[r * LDA + r]);
+        for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+        const Real eps = max((Real)ridge * dmax, (Real)0);
+        for (int r = lane; r < R; r += 32) A[r * LDA + r] += eps;
+        __syncwarp();
+        // right-looking Cholesky; lane owns rows lane, lane + 32
+        for (int j = 0; j < R; ++j) {
+            // one reciprocal square root per pivot: d = s * rsqrt(s), 1/d =
+            // rsqrt(s) (a serial chain of 2R FP64 divides and square roots
+            // is most of this kernel's time otherwise)
+            Real inv = 0;
+            if (lane == (j & 31)) {
+                Real sj = A[j * LDA + j];
+                if (sj < (Real)0) sj = 0;
+                const Real rs = sj > (Real)0 ? rsqrt(sj) : (Real)0;
+                A[j * LDA + j] = sj * rs;
+                inv = rs;
+                invd[j] = rs;
+            }
+            inv = __shfl_sync(0xffffffffu, inv, j & 31);
+            for (int i = j + 1 + ((lane - j - 1) & 31); i < R; i += 32) A[i * LDA + j] *= inv;
+            __syncwarp();
+            for (int i = j + 1 + ((lane - j - 1) & 31); i < R; i += 32) {
+                const Real aij = A[i * LDA + j];
+                for (int k = j + 1; k <= i; ++k) A[i * LDA + k] -= aij * A[k * LDA + j];
+            }
+            __syncwarp();
+        }
+        // W[c][:] = solve(e_c): lane owns columns c = lane, lane + 32; the
+        // inner products use four partial sums to shorten the FMA chains
+        for (int c = lane; c < R; c += 32) {
+            // x_c[r] lives at Wx[r * R + c]: the lanes of one access are
+            // consecutive doubles (no bank conflicts)
+            double* xc = Wx + c;
+#define X(r) xc[(size_t)(r) * R]
+            for (int r = 0; r < R; ++r) X(r) = (r == c) ? 1.0 : 0.0;
+            for (int r = 0; r < R; ++r) {
+                Real s0 = (Real)X(r), s1 = 0, s2 = 0, s3 = 0;
+                int k = 0;
+                for (; k + 4 <= r; k += 4) {
+                    s0 -= A[r * LDA + k] * (Real)X(k);
+                    s1 -= A[r * LDA + k + 1] * (Real)X(k + 1);
+                    s2 -= A[r * LDA + k + 2] * (Real)X(k + 2);
+                    s3 -= A[r * LDA + k + 3] * (Real)X(k + 3);
+                }
+                for (; k < r; ++k) s0 -= A[r * LDA + k] * (Real)X(k);
+                const Real sr = (s0 + s1) + (s2 + s3);
+                X(r) = (double)(sr * invd[r]);
+            }
+            for (int r = R - 1; r >= 0; --r) {
+                Real s0 = (Real)X(r), s1 = 0, s2 = 0, s3 = 0;
+                int k = r + 1;
+                for (; k + 4 <= R; k += 4) {
+                    s0 -= A[k * LDA + r] * (Real)X(k);
+                    s1 -= A[(k + 1) * LDA + r] * (Real)X(k + 1);
+                    s2 -= A[(k + 2) * LDA + r] * (Real)X(k + 2);
+                    s3 -= A[(k + 3) * LDA + r] * (Real)X(k + 3);
+                }
+                for (; k < R; ++k) s0 -= A[k * LDA + r] * (Real)X(k);
+                const Real sr = (s0 + s1) + (s2 + s3);
+                X(r) = (double)(sr * invd[r]);
+            }
+#undef X
+        }
+    }
+    __syncthreads();
+    // Y = Yhat W (padding columns zero)
+    for (uint32_t e = tid; e < total; e += nt) {
+        const uint32_t i = e / Rp;
+        const int c = (int)(e - i * Rp);
+        if (c >= R) { Ys[e] = 0.f; continue; }
+        const float* yh = Hs + (size_t)i * Rp;
+        Real a0 = 0, a1 = 0;
+        int k = 0;
+        for (; k + 2 <= R; k += 2) {
+            a0 += (Real)yh[k] * (Real)Wx[k * R + c];
+            a1 += (Real)yh[k + 1] * (Real)Wx[(k + 1) * R + c];
+        }
+        if (k < R) a0 += (Real)yh[k] * (Real)Wx[k * R + c];
+        Ys[e] = (float)(a0 + a1);
+    }
+    __syncthreads();
+    // Gram of Y in FP64: thread = (entry, row slice)
+    {
+        const int slices = max(1, nt / RR);
+        const int pe = tid % RR, sl = tid / RR;
+        if (sl < slices && tid < RR * slices) {
+            const int a = pe / R, b = pe % R;
+            double acc = 0.0;
+            for (uint32_t i = sl; i < rows; i += slices)
+                acc += (double)Ys[(size_t)i * Rp + a] * (double)Ys[(size_t)i * Rp + b];
+            atomicAdd(&G[pe], acc);
+        }
+        for (int e = tid + nt; e < RR; e += nt) {      // RR > nt: remaining entries
+            const int a = e / R, b = e % R;
+            double acc = 0.0;
+            for (uint32_t i = 0; i < rows; ++i)
+                acc += (double)Ys[(size_t)i * Rp + a] * (double)Ys[(size_t)i * Rp + b];
+            G[e] = acc;
+        }
+    }
+    __syncthreads();
+    for (int r = tid; r < R; r += nt) {
+        const double l = sqrt(max(G[r * R + r], 0.0));
+        lam[r] = l;
+        lam64[r] = l;
+        lambda[r] = (float)l;
+    }
+    __syncthreads();
+    for (int e = tid; e < RR; e += nt) {
+        const double la = lam[e / R], lb = lam[e % R];
+        const double ia = la > 1e-20 ? 1.0 / la : 0.0, ib = lb > 1e-20 ? 1.0 / lb : 0.0;
+        const double g = G[e] * ia * ib;
+        Gd[(size_t)n * RR + e] = g;
+        G32[(size_t)n * RR + e] = (float)g;
+    }
+    for (uint32_t e = tid; e < total; e += nt) {
+        const int c = (int)(e % Rp);
+        if (c >= R) { Y[e] = 0.f; continue; }
+        const double l = lam[c];
+        const float inv = l > 1e-20 ? (float)(1.0 / l) : 0.f;
+        const float y = Ys[e] * inv;
+        Y[e] = y;
+        if (last) atomicAdd(&dot[c], (double)y * (double)Hs[e]);
+    }
+    __syncthreads();
+    if (!last) return;
+    // fit: <T,M> = sum_r lambda_r <Y_r, Yhat_r>, ||M||^2 from the Grams
+    double s_in = 0.0, s_m = 0.0;
+    for (int r = tid; r < R; r += nt) s_in += lam[r] * dot[r];
+    for (int e = tid; e < RR; e += nt) {
+        double h = 1.0;
+        for (int m = 0; m < N; ++m) h *= Gd[(size_t)m * RR + e];
+        s_m += lam[e / R] * lam[e % R] * h;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s_in += __shfl_xor_sync(0xffffffffu, s_in, o);
+        s_m += __shfl_xor_sync(0xffffffffu, s_m, o);
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    __shared__ double red2[32];
+    if (lane == 0) { red[warp] = s_in; red2[warp] = s_m; }
+    __syncthreads();
+    if (tid == 0) {
+        double inner = 0.0, m2 = 0.0;
+        for (int w = 0; w < nt / 32; ++w) { inner += red[w]; m2 += red2[w]; }
+        m2 = max(0.0, m2);
+        double r2 = tnorm2 - 2.0 * inner + m2;
+        if (r2 < 0.0) r2 = 0.0;
+        const double resid = sqrt(r2);
+        fitout[0] = inner;
+        fitout[1] = m2;
+        fitout[2] = 1.0 - resid / max(sqrt(tnorm2), 1e-30);
+        fitout[3] = resid;
+    }
+}
+
+// Device-side loop control of graph-replayed CP-ALS: records the iteration's
+// fit and residual and keeps the WHILE condition set until the reference's
+// stop rule (|fit_i - fit_{i-1}| < tol after the first iteration,
+// src/dynasor_cpals.cpp:371-379) or max_iters ends the loop.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const double* __restrict__ fitout,
+                           double* __restrict__ st, double* __restrict__ fit_hist,
+                           double* __restrict__ resid_hist, double tol, int max_iters)
+{
+    if (threadIdx.x != 0) return;
+    const int it = (int)st[0];
+    const double fit = fitout[2];
+    fit_hist[it] = fit;
+    resid_hist[it] = fitout[3];
+    const bool stop = (it > 0 && fabs(fit - st[1]) < tol) || (it + 1 >= max_iters);
+    st[1] = fit;
+    st[0] = (double)(it + 1);
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
 __global__ void k_sumsq(const float* __restrict__ v, uint64_t n, double* __restrict__ out) {
     __shared__ double red[256];
     double s = 0;
@@ -373,9 +594,41 @@ unsigned grid_for(size_t work, unsigned cap = 148 * 8) {
     return (unsigned)std::max<size_t>(1, std::min<size_t>((work + kLaThreads - 1) / kLaThreads, cap));
 }
 
-// One ALS factor update of mode n from Yhat[n] (cpals.cpp:290-321).
-int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge, bool last) {
+size_t small_update_smem(int R, int Rp, uint32_t rows, bool fp64) {
+    const size_t RR = (size_t)R * R;
+    return (2 * RR + 2 * (size_t)R) * sizeof(double) +
+           (size_t)R * (R + 2) * (fp64 ? sizeof(double) : sizeof(float)) +
+           2 * (size_t)rows * Rp * sizeof(float);
+}
+
+// One ALS factor update of mode n from Yhat[n] (cpals.cpp:290-321).  For the
+// last mode *fit_done reports whether the fit was computed with it.
+int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge, bool last,
+                double tn2, bool* fit_done) {
     const size_t RR = (size_t)p.R * p.R;
+    *fit_done = false;
+    if (p.R <= 64 && (uint64_t)p.dims[n] * p.Rp <= 8192 && (uint64_t)p.dims[n] * RR <= (1ull << 21)) {
+        const size_t sm = small_update_smem(p.R, p.Rp, p.dims[n], solve_fp64 != 0);
+        if (solve_fp64) {
+            if (sm > 48 * 1024)
+                DGPU_CUDA(cudaFuncSetAttribute(k_update_small<double>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_update_small<double><<<1, 1024, sm, p.stream>>>(
+                L.Gd, L.G32, p.N, n, p.R, p.Rp, ridge, p.Yhat[n], p.Y[n], p.dims[n], p.lambda,
+                L.lam64, last ? 1 : 0, tn2, L.fitout);
+        } else {
+            if (sm > 48 * 1024)
+                DGPU_CUDA(cudaFuncSetAttribute(k_update_small<float>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_update_small<float><<<1, 1024, sm, p.stream>>>(
+                L.Gd, L.G32, p.N, n, p.R, p.Rp, ridge, p.Yhat[n], p.Y[n], p.dims[n], p.lambda,
+                L.lam64, last ? 1 : 0, tn2, L.fitout);
+        }
+        DGPU_CUDA(cudaGetLastError());
+        p.yb_stale[n] = true;
+        *fit_done = last;
+        return DGPU_OK;
+    }
     if (solve_fp64) {
         k_build_solve_map<double><<<1, 1024, 0, p.stream>>>(L.Gd, p.N, n, p.R, ridge, L.A, L.Wd, L.W32);
         const size_t sm = RR * sizeof(double);
@@ -461,42 +714,214 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
                     "tol=%.1e  seed=%llu\n", p.N, p.R, p.Rp, (unsigned long long)p.nnz,
                     res.tensor_norm, o.max_iters, o.tol, (unsigned long long)o.seed);
 
-    cudaEvent_t ev[4];
-    for (auto& e : ev) DGPU_CUDA(cudaEventCreate(&e));
+    // Events: ev[0] iteration start, ev[1 + 2n] end of mode n's MTTKRP,
+    // ev[2 + 2n] end of its factor update (Jacobi: ev[1] ends the all-modes
+    // MTTKRP and ev[2 + 2n] each update).
     const bool jacobi = (o.kernel == DGPU_CP_JACOBI);
-    double fit_prev = 0.0;
-    const auto t_start = clk::now();
-    for (int it = 0; it < o.max_iters; ++it) {
-        const auto t_it = clk::now();
-        float mt_ms = 0.f, la_ms = 0.f;
-        if (jacobi) {
-            DGPU_CUDA(cudaEventRecord(ev[0], p.stream));
+    const int nev = 2 * p.N + 2;
+    std::vector<cudaEvent_t> ev(nev, nullptr);
+    for (auto& e : ev) DGPU_CUDA(cudaEventCreate(&e));
+    double* fit_host = nullptr;              // pinned: the graph's D2H target
+    DGPU_CUDA(cudaMallocHost((void**)&fit_host, 4 * sizeof(double)));
+    struct Cleanup {
+        std::vector<cudaEvent_t>& ev; double* fh; cudaGraphExec_t* ex;
+        ~Cleanup() {
+            for (auto e : ev) if (e) cudaEventDestroy(e);
+            if (fh) cudaFreeHost(fh);
+            for (int k = 0; k < 2; ++k) if (ex[k]) cudaGraphExecDestroy(ex[k]);
+        }
+    };
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int cur_after[2] = {0, 0};
+    Cleanup cleanup{ev, fit_host, exec};
+
+    // One iteration's work on p.stream.  kind 0: eager; 1: captured for
+    // per-iteration replay (event records become graph event nodes); 2: the
+    // body of the device-side loop (no events, no host copy; the loop
+    // control kernel follows).
+    auto enqueue = [&](int kind) -> int {
+        auto rec = [&](int i) -> cudaError_t {
+            if (kind == 2) return cudaSuccess;
+            return kind == 1 ? cudaEventRecordWithFlags(ev[i], p.stream, cudaEventRecordExternal)
+                             : cudaEventRecord(ev[i], p.stream);
+        };
+        DGPU_CUDA(rec(0));
+        bool fit_done = false;
+        if (jacobi)
             DGPU_TRY(launch_mttkrp_all_modes(p, p.layout == DGPU_LAYOUT_NCOPY ? p.slab[0]
                                                                               : p.slab[p.cur]));
-            DGPU_CUDA(cudaEventRecord(ev[1], p.stream));
-            DGPU_CUDA(cudaEventSynchronize(ev[1]));
-            cudaEventElapsedTime(&mt_ms, ev[0], ev[1]);
-        }
         for (int n = 0; n < p.N; ++n) {
-            DGPU_CUDA(cudaEventRecord(ev[0], p.stream));
             if (!jacobi)
                 DGPU_TRY(p.layout == DGPU_LAYOUT_NCOPY ? mode_ncopy(p, n) : mode_pingpong(p, n));
-            DGPU_CUDA(cudaEventRecord(ev[1], p.stream));
-            DGPU_TRY(update_mode(p, L, n, o.solve_fp64, o.ridge, n == p.N - 1));
-            DGPU_CUDA(cudaEventRecord(ev[2], p.stream));
-            DGPU_CUDA(cudaEventSynchronize(ev[2]));
+            DGPU_CUDA(rec(1 + 2 * n));
+            DGPU_TRY(update_mode(p, L, n, o.solve_fp64, o.ridge, n == p.N - 1, tn2, &fit_done));
+            DGPU_CUDA(rec(2 + 2 * n));
+        }
+        if (!fit_done) {
+            const int nblk = (int)grid_for((size_t)p.dims[p.N - 1] * p.Rp, kGramChunks);
+            k_fit<<<1, 1024, 0, p.stream>>>(L.Gd, p.N, p.R, L.lam64, L.dot, nblk, tn2, L.fitout);
+            DGPU_CUDA(cudaGetLastError());
+        }
+        if (kind != 2)
+            DGPU_CUDA(cudaMemcpyAsync(fit_host, L.fitout, 4 * sizeof(double),
+                                      cudaMemcpyDeviceToHost, p.stream));
+        return DGPU_OK;
+    };
+
+    // Runs iterations first.. on the device; returns the number run in *done.
+    auto device_loop = [&](int first, double fit_before, int* done) -> int {
+        *done = 0;
+        const int left = o.max_iters - first;
+        if (left <= 0) return DGPU_OK;
+        double* st = nullptr;        // [it, fit_prev] + fit and residual histories
+        DGPU_TRY(dev_alloc(p, (void**)&st, (2 + 2 * (size_t)o.max_iters) * sizeof(double)));
+        struct Free { double* q; Plan& pl; size_t b;
+                      ~Free() { dev_free(q); pl.device_bytes -= b; } }
+            fr{st, p, (2 + 2 * (size_t)o.max_iters) * sizeof(double)};
+        const double init[2] = {(double)first, fit_before};
+        DGPU_CUDA(cudaMemcpyAsync(st, init, sizeof(init), cudaMemcpyHostToDevice, p.stream));
+        DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        cudaGraph_t outer = nullptr;
+        cudaGraphExec_t gx = nullptr;
+        struct G { cudaGraph_t& g; cudaGraphExec_t& x;
+                   ~G() { if (x) cudaGraphExecDestroy(x); if (g) cudaGraphDestroy(g); } } gg{outer, gx};
+        DGPU_CUDA(cudaGraphCreate(&outer, 0));
+        cudaGraphConditionalHandle h;
+        DGPU_CUDA(cudaGraphConditionalHandleCreate(&h, outer, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        DGPU_CUDA(cudaGraphAddNode(&node, outer, nullptr, 0, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        const int cur0 = p.cur, nm0 = p.next_mode;
+        bool stale0[kMaxModes];
+        for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
+        auto restore = [&]() {
+            p.cur = cur0;
+            p.next_mode = nm0;
+            for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
+        };
+        if (cudaStreamBeginCaptureToGraph(p.stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cpals: device loop capture not available; iterating from the host");
+            return DGPU_ERR_CUDA;
+        }
+        int rc = enqueue(2);
+        if (rc == DGPU_OK) {
+            k_loop_ctl<<<1, 32, 0, p.stream>>>(h, L.fitout, st, st + 2, st + 2 + o.max_iters,
+                                               o.tol, o.max_iters);
+            if (cudaGetLastError() != cudaSuccess) rc = DGPU_ERR_CUDA;
+        }
+        cudaGraph_t cap = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(p.stream, &cap);
+        if (rc != DGPU_OK || ec != cudaSuccess || cudaGraphInstantiate(&gx, outer, 0) != cudaSuccess) {
+            cudaGetLastError();
+            restore();
+            if (rc != DGPU_OK && rc != DGPU_ERR_CUDA) return rc;
+            set_error("cpals: device loop graph not available; iterating from the host");
+            return DGPU_ERR_CUDA;
+        }
+        DGPU_CUDA(cudaEventRecord(ev[0], p.stream));
+        DGPU_CUDA(cudaGraphLaunch(gx, p.stream));
+        DGPU_CUDA(cudaEventRecord(ev[1], p.stream));
+        DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        std::vector<double> hs(2 + 2 * (size_t)o.max_iters);
+        DGPU_CUDA(cudaMemcpy(hs.data(), st, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        const int last = (int)hs[0];           // iterations completed so far
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        // the loop's device time, split between MTTKRP and the factor
+        // updates in the proportion measured on the first (eager) iteration
+        const double tot = res.mttkrp_time_s + res.linalg_time_s;
+        const double fm = tot > 0 ? res.mttkrp_time_s / tot : 0.5;
+        res.mttkrp_time_s += fm * ms * 1e-3;
+        res.linalg_time_s += (1.0 - fm) * ms * 1e-3;
+        for (int i = first; i < last; ++i) {
+            if (fit_history) fit_history[i] = hs[2 + i];
+            res.final_fit = hs[2 + i];
+            res.final_residual = hs[2 + o.max_iters + i];
+        }
+        res.iters_done = last;
+        *done = last - first;
+        return DGPU_OK;
+    };
+
+    // Graph replay: the launches of an iteration depend only on which slab
+    // holds the mode-0 order when it starts (PingPong), so at most two graphs
+    // are captured; host-side plan state is advanced as the capture left it.
+    bool graphs = o.graphs != 0 && !p.timing;
+    double fit_prev = 0.0;
+    const auto t_start = clk::now();
+    const int cur_start = p.cur;
+    for (int it = 0; it < o.max_iters; ++it) {
+        const auto t_it = clk::now();
+        const int key = (p.layout == DGPU_LAYOUT_NCOPY) ? 0 : (p.cur & 1);
+        // After the first (eager) iteration, when an iteration leaves the
+        // live slab where it found it, the remaining iterations run as one
+        // graph launch: a device-side WHILE loop whose body is one iteration
+        // plus a control kernel that records the fit and applies the
+        // reference's stop rule (no host round trip per iteration).
+        if (graphs && it == 1 && !o.verbose &&
+            (p.layout == DGPU_LAYOUT_NCOPY || p.cur == cur_start)) {
+            int done = 0;
+            const int rc = device_loop(it, fit_prev, &done);
+            if (rc == DGPU_OK && done > 0) break;
+            if (rc != DGPU_OK && rc != DGPU_ERR_CUDA) return rc;
+            graphs = rc == DGPU_OK;      // capture unsupported: continue eagerly
+        }
+        if (graphs && it > 0 && exec[key]) {
+            DGPU_CUDA(cudaGraphLaunch(exec[key], p.stream));
+            p.cur = cur_after[key];
+            p.next_mode = 0;
+        } else if (graphs && it > 0) {
+            // capturing advances the host-side plan state (live slab, next
+            // mode, BF16 mirror flags) without running the work; keep the
+            // state to restore it if the capture cannot be used
+            const int cur0 = p.cur, nm0 = p.next_mode;
+            bool stale0[kMaxModes];
+            for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
+            cudaGraph_t g = nullptr;
+            cudaError_t ec = cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeRelaxed);
+            int rc = DGPU_OK;
+            if (ec == cudaSuccess) {
+                rc = enqueue(1);
+                ec = cudaStreamEndCapture(p.stream, &g);
+            }
+            cudaError_t ei = cudaErrorUnknown;
+            if (rc == DGPU_OK && ec == cudaSuccess && g)
+                ei = cudaGraphInstantiate(&exec[key], g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (rc == DGPU_OK && ec == cudaSuccess && ei == cudaSuccess) {
+                cur_after[key] = p.cur;
+                DGPU_CUDA(cudaGraphLaunch(exec[key], p.stream));
+            } else {
+                // this stream cannot be captured (e.g. the legacy default
+                // stream): iterate eagerly from here on
+                cudaGetLastError();
+                exec[key] = nullptr;
+                graphs = false;
+                p.cur = cur0;
+                p.next_mode = nm0;
+                for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
+                DGPU_TRY(enqueue(0));
+            }
+        } else {
+            DGPU_TRY(enqueue(0));
+        }
+        DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        float mt_ms = 0.f, la_ms = 0.f;
+        for (int n = 0; n < p.N; ++n) {
             float a = 0.f, b = 0.f;
-            cudaEventElapsedTime(&a, ev[0], ev[1]);
-            cudaEventElapsedTime(&b, ev[1], ev[2]);
+            cudaEventElapsedTime(&a, ev[n == 0 ? 0 : 2 * n], ev[1 + 2 * n]);
+            cudaEventElapsedTime(&b, ev[1 + 2 * n], ev[2 + 2 * n]);
             mt_ms += a;
             la_ms += b;
         }
-        const int nblk = (int)grid_for((size_t)p.dims[p.N - 1] * p.Rp, kGramChunks);
-        k_fit<<<1, 1024, 0, p.stream>>>(L.Gd, p.N, p.R, L.lam64, L.dot, nblk, tn2, L.fitout);
-        DGPU_CUDA(cudaGetLastError());
-        double fo[4];
-        DGPU_CUDA(cudaMemcpyAsync(fo, L.fitout, sizeof(fo), cudaMemcpyDeviceToHost, p.stream));
-        DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        const double* fo = fit_host;
         const double fit = fo[2];
         res.mttkrp_time_s += mt_ms * 1e-3;
         res.linalg_time_s += la_ms * 1e-3;
@@ -517,7 +942,6 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
         fit_prev = fit;
     }
     res.total_time_s = std::chrono::duration<double>(clk::now() - t_start).count();
-    for (auto& e : ev) cudaEventDestroy(e);
     if (o.verbose)
         std::printf("[cpals] done  iters=%d  final_fit=%.6f  resid=%.3e\n"
                     "[cpals] total = %.3f s   spMTTKRP = %.3f s (%.1f%%)   linalg  = %.3f s (%.1f%%)\n",

@@ -136,7 +136,15 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     const int grp = lane / G, gl = lane % G;
     const int C4 = Rp >> 2;
 
-    const Tile tl = tiles[blockIdx.x];
+    // a tile may be split over gridDim.y CTAs (small tensors: more CTAs);
+    // row runs cut at a split point are flushed with atomics like any other
+    Tile tl = tiles[blockIdx.x];
+    if (gridDim.y > 1) {
+        const uint32_t a = (uint32_t)(((uint64_t)tl.count * blockIdx.y) / gridDim.y);
+        const uint32_t b = (uint32_t)(((uint64_t)tl.count * (blockIdx.y + 1)) / gridDim.y);
+        tl.begin += a;
+        tl.count = b - a;
+    }
     const uint32_t per_w = (tl.count + kRunWarps - 1) / kRunWarps;
     const uint32_t wb = min(tl.count, (uint32_t)warp * per_w);
     const uint32_t we = min(tl.count, wb + per_w);
@@ -430,9 +438,13 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
     const int C4 = p.Rp / 4;
     const SlabPtrs sp = slab_in(in, p.N);
     float* out = p.Yhat[n];
+    // at least ~4 CTAs per SM: split tiles when the tensor has few of them
+    const uint32_t want = 4u * (uint32_t)p.sms;
+    const uint32_t split = ntiles >= want ? 1u : std::min(16u, (want + ntiles - 1) / std::max(1u, ntiles));
+    const dim3 grid(ntiles, split);
 #define DGPU_RUNT(G, V, TN)                                                                      \
-    k_mttkrp_rowrun<N, G, V, BF, TN><<<ntiles, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, \
-                                                                           w0, wl, p.Rp)
+    k_mttkrp_rowrun<N, G, V, BF, TN><<<grid, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, \
+                                                                         w0, wl, p.Rp)
 #define DGPU_RUN(G, V) DGPU_RUNT(G, V, -1)
     // target-mode specialisations for the common 3- and 4-mode, Rp <= 128 shapes
 #define DGPU_RUN_TGT(G)                                                       \

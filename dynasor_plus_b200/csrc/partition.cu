@@ -46,7 +46,16 @@ namespace dgpu {
 namespace {
 
 constexpr int kHistThreads = 1024;
-constexpr int kScatThreads = 512;
+#ifndef DGPU_SCAT_THREADS
+#define DGPU_SCAT_THREADS 512
+#endif
+#ifndef DGPU_SCAT_WINDOW
+#define DGPU_SCAT_WINDOW 2048
+#endif
+#ifndef DGPU_SCAT_MINB
+#define DGPU_SCAT_MINB 2
+#endif
+constexpr int kScatThreads = DGPU_SCAT_THREADS;   // threads of a scatter CTA
 constexpr int kScatWarps = kScatThreads / 32;
 constexpr uint32_t kSegChunkTiles = 16;       // <= 64K elements per segmented chunk
 
@@ -235,7 +244,7 @@ __device__ __forceinline__ void issue_window(uint32_t* buf, const SlabPtrs& in, 
 // columns; staging needs a 16-byte record + destination (5 words) when
 // N <= 3, else N+2 columns.
 template <int N>
-constexpr int scatter_window() { return N <= 4 ? 2048 : 1024; }
+constexpr int scatter_window() { return N <= 4 ? DGPU_SCAT_WINDOW : DGPU_SCAT_WINDOW / 2; }
 template <int N>
 constexpr int scatter_cols() { return N + 1 <= 4 ? 5 : N + 2; }
 
@@ -252,7 +261,7 @@ constexpr int scatter_cols() { return N + 1 <= 4 ? 5 : N + 2; }
 //   d. the staged window is written out: consecutive threads store
 //      consecutive slots of one bucket.
 template <int N, int W>
-__global__ void __launch_bounds__(kScatThreads, 2)
+__global__ void __launch_bounds__(kScatThreads, DGPU_SCAT_MINB)
 k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
                 const Tile* __restrict__ tiles, const Chunk* __restrict__ chunks,
                 const uint32_t* __restrict__ order, uint32_t nchunks,
@@ -267,7 +276,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     constexpr bool kRec = (N + 1 <= 4);
     constexpr int C = scatter_cols<N>();          // buffer columns (input, then stage)
     constexpr int DC = kRec ? 4 : N + 1;          // column holding staged destinations
-    constexpr int BPT = kMaxBuckets / kScatThreads;   // buckets per thread, at most
+    constexpr int BPT = (kMaxBuckets + kScatThreads - 1) / kScatThreads;  // buckets per thread, at most
     extern __shared__ __align__(128) uint32_t sm[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t wsum[kScatWarps];
@@ -495,13 +504,18 @@ int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, 
 {
     constexpr int W = scatter_window<N>();
     const size_t smem = scatter_smem<N>(nb);
-    static uint64_t attr_set = 0;          // per device (function attributes are per context)
-    const uint64_t dbit = 1ull << (p.device & 63);
-    if (!(attr_set & dbit)) {
+    // dynamic shared memory limit, raised per device (function attributes are
+    // per context) to the largest request seen so far
+    static size_t attr_bytes[64] = {};
+    size_t& have = attr_bytes[p.device & 63];
+    if (smem > have) {
+        if (smem > 227u * 1024u) {
+            set_error("stable_partition: %u buckets need %zu bytes of shared memory", nb, smem);
+            return DGPU_ERR_ARG;
+        }
         DGPU_CUDA(cudaFuncSetAttribute(k_chunk_scatter<N, W>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)scatter_smem<N>(kMaxBuckets)));
-        attr_set |= dbit;
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        have = smem;
     }
     int per_sm = 0;
     DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chunk_scatter<N, W>,

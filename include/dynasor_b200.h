@@ -121,6 +121,9 @@ typedef struct {
     int       solve_fp64;         /* 1: FP64 Cholesky + solve (default)   */
     int       use_init;           /* 1: start from the uploaded factors   */
     int       verbose;            /* print the reference's [cpals] lines  */
+    int       graphs;             /* 1: iterations after the first are
+                                     captured once as a CUDA graph and
+                                     replayed (default); 0: launch eagerly */
 } dgpu_cp_options;
 
 typedef struct {

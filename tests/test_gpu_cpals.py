@@ -73,3 +73,62 @@ def test_jacobi_matches_fp64_jacobi_oracle(bindings):
     assert np.max(np.abs(r["fit_history"] - fit64)) < 1e-3
     for n in range(len(dims)):
         assert rel_fro(p.factor(n)[:, :R], Y64[n][:, :R]) < 1e-2
+
+
+@pytest.mark.parametrize("layout,kernel", [("pingpong", "gs"), ("ncopy", "gs"), ("pingpong", "jacobi")])
+def test_graph_replay_matches_eager_iterations(layout, kernel):
+    """Iterations replayed from a captured CUDA graph give the eager fit
+    trajectory and factors (only atomic summation order may differ).  The
+    Jacobi iteration amplifies such rounding differences from one step to
+    the next (it does not converge on this tensor), so it is compared over
+    its first three iterations."""
+    import dynasor_plus_b200 as d
+    g = load_golden("ref_cpals_r5.npz")
+    dims = g["dims"]
+    idx = [g[f"idx{n}"] for n in range(len(dims))]
+    iters = 3 if kernel == "jacobi" else 12
+    out = []
+    for graphs in (False, True):
+        p = d.Plan(dims, g["vals"], idx, threads=int(g["T"]), rank=int(g["R"]), layout=layout)
+        r = p.cpals(max_iters=iters, tol=0.0, seed=42, kernel=kernel, graphs=graphs)
+        out.append((r["fit_history"], [p.factor(n) for n in range(len(dims))]))
+        p.close()
+    assert len(out[0][0]) == len(out[1][0]) == iters
+    assert np.max(np.abs(out[0][0] - out[1][0])) < (1e-5 if kernel == "jacobi" else 1e-6)
+    for a, b in zip(out[0][1], out[1][1]):
+        assert rel_fro(b, a) < (1e-4 if kernel == "jacobi" else 1e-5)
+
+
+@pytest.mark.parametrize("solve_fp64", [True, False])
+def test_large_and_small_mode_updates_match_fp64_oracle(bindings, solve_fp64):
+    """Mode 0 (40,000 rows x rank 16) takes the multi-kernel factor update,
+    modes 1-2 the single-CTA one; the trajectory follows the FP64 oracle."""
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.cp_truth((40_000, 300, 200), 200_000, 5, 0.01, seed=7)
+    R, it = 16, 6
+    p = d.Plan(dims, vals, idx, threads=8, rank=R)
+    r = p.cpals(max_iters=it, tol=0.0, seed=42, solve_fp64=solve_fp64)
+    fit64, Y64, lam64 = bindings.cpals_f64(dims, vals, idx, R, it, 0.0, seed=42)
+    assert np.max(np.abs(r["fit_history"] - fit64)) < (1e-6 if solve_fp64 else 1e-4)
+    for n in range(len(dims)):
+        assert rel_fro(p.factor(n)[:, :R], Y64[n][:, :R]) < (1e-4 if solve_fp64 else 1e-2)
+    p.close()
+
+
+@pytest.mark.parametrize("layout", ["pingpong", "ncopy"])
+def test_device_loop_stop_rule_matches_host_loop(layout):
+    """The device-side loop (graph replay with a WHILE condition) stops at
+    the same iteration as the host loop and records the same fits."""
+    import dynasor_plus_b200 as d
+    g = load_golden("ref_cpals_r5.npz")
+    dims = g["dims"]
+    idx = [g[f"idx{n}"] for n in range(len(dims))]
+    res = []
+    for graphs in (False, True):
+        p = d.Plan(dims, g["vals"], idx, threads=int(g["T"]), rank=int(g["R"]), layout=layout)
+        res.append(p.cpals(max_iters=50, tol=1e-4, seed=42, graphs=graphs))
+        p.close()
+    assert res[0]["iters_done"] == res[1]["iters_done"]
+    assert np.max(np.abs(res[0]["fit_history"] - res[1]["fit_history"])) < 1e-6
+    assert abs(res[0]["final_fit"] - res[1]["final_fit"]) < 1e-6
