@@ -147,6 +147,41 @@ def make_workload(args, device="cuda"):
     return synth.zipf(DIMS, args.draws, ZIPF_S, SEED)
 
 
+def cpals_small_workload():
+    """The plain CP-ALS configuration: 200 x 200 x 200, 100,000 distinct
+    uniform coordinates, rank-5 U(0,1) truth + 1% Gaussian noise; rank 16,
+    50 Gauss-Seidel iterations, tol 1e-4, seed 42 (synthetic, seeded)."""
+    from dynasor_plus_b200 import synth
+    return synth.cp_truth((200, 200, 200), 100_000, 5, 0.01, seed=1)
+
+
+def cpals_small_gpu(threads):
+    """CP-ALS iterations/s on the small configuration, both layouts."""
+    import dynasor_plus_b200 as d
+    dims, vals, idx = cpals_small_workload()
+    out = {}
+    for layout in ("ncopy", "pingpong"):
+        p = d.Plan(dims, vals, idx, threads=threads, rank=16, layout=layout)
+        p.cpals(max_iters=50, tol=1e-4, seed=42)          # warm-up
+        r = p.cpals(max_iters=50, tol=1e-4, seed=42)
+        out[layout] = {"iters": r["iters_done"], "iter_per_s": r["iters_done"] / r["total_time_s"],
+                       "final_fit": r["final_fit"]}
+        p.close()
+    return out
+
+
+def cpals_small_reference(threads):
+    from oracle import bindings as B
+    dims, vals, idx = cpals_small_workload()
+    out = {}
+    for layout in ("ncopy", "pingpong"):
+        ref = B.Reference(dims, vals, idx)
+        ref.build(threads, layout)
+        fit, lam, tot, mt = ref.cpals(16, 50, 1e-4, 42)
+        out[layout] = {"iters": len(fit), "iter_per_s": len(fit) / tot, "final_fit": float(fit[-1])}
+    return out
+
+
 def uniform_factors(dims, R, seed=42):
     rng = np.random.default_rng(seed)
     Rp = (R + 15) // 16 * 16
@@ -227,6 +262,11 @@ def run_reference_arm(args):
                          "sample": f"random {nnz} of {len(vals)} nonzeros, same dims"},
         "e2e": {"value": val, "unit": "GNNZ/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        out["cpals_small"] = {"workload": "200x200x200, 100k nnz, rank 16, GS, tol 1e-4",
+                              "threads": cores, **cpals_small_reference(cores)}
+    except Exception as ex:  # reported, never required
+        out["cpals_small"] = {"error": str(ex)[:200]}
     print(json.dumps(out))
 
 
@@ -385,12 +425,16 @@ def main():
         "clocks": clocks,
     }
 
-    # CP-ALS iterations/s on the same tensor (Gauss-Seidel, FP64 solve)
+    # CP-ALS iterations/s on the same tensor (Gauss-Seidel, FP64 solve) and
+    # on the small plain CP-ALS configuration
     if args.cpals_iters > 0:
         r = plan.cpals(max_iters=args.cpals_iters, tol=0.0, seed=42)
         out["cpals"] = {"iters": r["iters_done"], "iter_per_s": r["iters_done"] / r["total_time_s"],
                         "final_fit": r["final_fit"], "mttkrp_s": r["mttkrp_time_s"],
                         "linalg_s": r["linalg_time_s"]}
+        if rank == 0:
+            out["cpals_small"] = {"workload": "200x200x200, 100k nnz, rank 16, GS, tol 1e-4",
+                                  "plan_threads": args.threads, **cpals_small_gpu(args.threads)}
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:

@@ -136,3 +136,28 @@ def zipf_torch(dims=(1_000_000, 200_000, 50_000), draws=100_000_000, s=1.1, seed
     vals = torch.empty(nnz, device=device, dtype=torch.float32).log_normal_(0.0, 1.0, generator=g)
     out_idx = [i.cpu().numpy().view(np.uint32) for i in idx]
     return np.asarray(dims_l, np.uint32), vals.cpu().numpy(), out_idx
+
+
+def cp_zipf_torch(dims=(50_000, 20_000, 2_000, 500), draws=200_000_000, s=(0, 0, 1.3, 1.3),
+                  rank=10, noise=0.05, seed=3, device="cuda"):
+    """Coordinates as ``zipf_torch`` (per-mode Zipf exponents, 0 = uniform),
+    values from a rank-`rank` CP model with |N(0,1)| factors plus Gaussian
+    noise with sigma = `noise` x mean value (the 4-mode mixed-precision
+    CP-ALS workload).  Returns host numpy arrays."""
+    import torch
+
+    dims, _, idx = zipf_torch(dims, draws, s, seed, device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 7)
+    U = [torch.randn((int(I), rank), generator=g, device=device).abs_() for I in dims]
+    v = None
+    for r in range(rank):
+        t = None
+        for n in range(len(dims)):
+            ix = torch.from_numpy(idx[n].view(np.int32)).to(device).long()
+            col = U[n][:, r][ix]
+            del ix
+            t = col if t is None else t * col
+        v = t if v is None else v + t
+    v = v + torch.randn(v.numel(), generator=g, device=device) * (noise * v.mean())
+    return dims, v.float().cpu().numpy(), idx
