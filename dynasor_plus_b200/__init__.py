@@ -261,6 +261,35 @@ class Plan:
             "lambda": self.lam(),
         }
 
+    def cpals_multistart(self, restarts, max_iters=50, tol=1e-4, seed=42, ridge=1e-10,
+                         kernel="gs", solve_fp64=True, use_init=False, verbose=False, graphs=True):
+        """`restarts` CP-ALS runs in this plan (rank = restarts x per-restart
+        rank); restart k starts from seed + k.  Returns one result dict per
+        restart; its factor columns are [k*Re, (k+1)*Re) of every factor."""
+        o = CpOptions()
+        lib().dgpu_cp_options_default(C.byref(o))
+        o.max_iters = int(max_iters)
+        o.tol = float(tol)
+        o.seed = int(seed)
+        o.ridge = float(ridge)
+        o.kernel = 1 if kernel in ("jacobi", "all-modes", "all_modes", "js") else 0
+        o.solve_fp64 = 1 if solve_fp64 else 0
+        o.use_init = 1 if use_init else 0
+        o.verbose = 1 if verbose else 0
+        o.graphs = 1 if graphs else 0
+        K = int(restarts)
+        res = (CpResult * K)()
+        hist = np.zeros((K, max(1, int(max_iters))), np.float64)
+        check(lib().dgpu_cpals_multistart(self._h, K, C.byref(o), C.cast(res, C.c_void_p),
+                                          hist.ctypes.data))
+        lam = self.lam()
+        Re = self.R // K
+        return [{"iters_done": r.iters_done, "final_fit": r.final_fit,
+                 "final_residual": r.final_residual, "tensor_norm": r.tensor_norm,
+                 "total_time_s": r.total_time_s,
+                 "fit_history": hist[k, :r.iters_done].copy(),
+                 "lambda": lam[k * Re:(k + 1) * Re].copy()} for k, r in enumerate(res)]
+
     def tensor_norm_sq(self) -> float:
         out = C.c_double(0)
         check(lib().dgpu_tensor_norm_sq(self._h, C.byref(out)))

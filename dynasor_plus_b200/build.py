@@ -48,7 +48,8 @@ def _newer(src: str, dst: str, deps) -> bool:
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+               glob.glob(os.path.join(ROOT, "include", "*.h")))
     cc = nvcc()
     objs, cmds = [], []
     for s in srcs:

@@ -16,6 +16,8 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o);
 int mode_pingpong(Plan& p, int n);
 int mode_ncopy(Plan& p, int n);
 int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& r, double* fit_history);
+int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_result* res,
+                         double* fit_history);
 }  // namespace dgpu
 
 using namespace dgpu;
@@ -383,6 +385,24 @@ int dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt, dgpu_cp_result* res,
     if (!opt || !res) { set_error("dgpu_cpals: null argument"); return DGPU_ERR_ARG; }
     if (opt->max_iters < 0) { set_error("dgpu_cpals: max_iters < 0"); return DGPU_ERR_ARG; }
     return cpals_run(*p, *opt, *res, fit_history);
+}
+
+int dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* opt,
+                          dgpu_cp_result* res, double* fit_history) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (!opt || !res) { set_error("dgpu_cpals_multistart: null argument"); return DGPU_ERR_ARG; }
+    if (opt->max_iters < 0) { set_error("dgpu_cpals_multistart: max_iters < 0"); return DGPU_ERR_ARG; }
+    if (restarts < 1 || p->R % restarts != 0) {
+        set_error("dgpu_cpals_multistart: the plan rank %d is not a multiple of %d restarts", p->R,
+                  restarts);
+        return DGPU_ERR_ARG;
+    }
+    if (p->R / restarts > 64) {
+        set_error("dgpu_cpals_multistart: rank per restart %d exceeds 64", p->R / restarts);
+        return DGPU_ERR_ARG;
+    }
+    return cpals_multistart_run(*p, restarts, *opt, res, fit_history);
 }
 
 }  // extern "C"

@@ -25,12 +25,14 @@
 //  Grams are kept in FP64 between modes.
 // ============================================================================
 #include "dgpu_internal.h"
+#include "la_warp.cuh"
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <random>
+#include <thread>
 #include <vector>
 
 namespace dgpu {
@@ -332,76 +334,9 @@ k_update_small(double* __restrict__ Gd, float* __restrict__ G32, int N, int n, i
     }
     for (int r = tid; r < R; r += nt) dot[r] = 0.0;
     __syncthreads();
-    // Ridge, Cholesky and the solve map run in warp 0 alone (warp barriers
-    // only); the other warps wait at the next block barrier.
-    if (tid < 32) {
-        const int lane = tid;
-        Real dmax = 0;
-        for (int r = lane; r < R; r += 32) dmax = max(dmax, A[r * LDA + r]);
-        for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-        const Real eps = max((Real)ridge * dmax, (Real)0);
-        for (int r = lane; r < R; r += 32) A[r * LDA + r] += eps;
-        __syncwarp();
-        // right-looking Cholesky; lane owns rows lane, lane + 32
-        for (int j = 0; j < R; ++j) {
-            // one reciprocal square root per pivot: d = s * rsqrt(s), 1/d =
-            // rsqrt(s) (a serial chain of 2R FP64 divides and square roots
-            // is most of this kernel's time otherwise)
-            Real inv = 0;
-            if (lane == (j & 31)) {
-                Real sj = A[j * LDA + j];
-                if (sj < (Real)0) sj = 0;
-                const Real rs = sj > (Real)0 ? rsqrt(sj) : (Real)0;
-                A[j * LDA + j] = sj * rs;
-                inv = rs;
-                invd[j] = rs;
-            }
-            inv = __shfl_sync(0xffffffffu, inv, j & 31);
-            for (int i = j + 1 + ((lane - j - 1) & 31); i < R; i += 32) A[i * LDA + j] *= inv;
-            __syncwarp();
-            for (int i = j + 1 + ((lane - j - 1) & 31); i < R; i += 32) {
-                const Real aij = A[i * LDA + j];
-                for (int k = j + 1; k <= i; ++k) A[i * LDA + k] -= aij * A[k * LDA + j];
-            }
-            __syncwarp();
-        }
-        // W[c][:] = solve(e_c): lane owns columns c = lane, lane + 32; the
-        // inner products use four partial sums to shorten the FMA chains
-        for (int c = lane; c < R; c += 32) {
-            // x_c[r] lives at Wx[r * R + c]: the lanes of one access are
-            // consecutive doubles (no bank conflicts)
-            double* xc = Wx + c;
-#define X(r) xc[(size_t)(r) * R]
-            for (int r = 0; r < R; ++r) X(r) = (r == c) ? 1.0 : 0.0;
-            for (int r = 0; r < R; ++r) {
-                Real s0 = (Real)X(r), s1 = 0, s2 = 0, s3 = 0;
-                int k = 0;
-                for (; k + 4 <= r; k += 4) {
-                    s0 -= A[r * LDA + k] * (Real)X(k);
-                    s1 -= A[r * LDA + k + 1] * (Real)X(k + 1);
-                    s2 -= A[r * LDA + k + 2] * (Real)X(k + 2);
-                    s3 -= A[r * LDA + k + 3] * (Real)X(k + 3);
-                }
-                for (; k < r; ++k) s0 -= A[r * LDA + k] * (Real)X(k);
-                const Real sr = (s0 + s1) + (s2 + s3);
-                X(r) = (double)(sr * invd[r]);
-            }
-            for (int r = R - 1; r >= 0; --r) {
-                Real s0 = (Real)X(r), s1 = 0, s2 = 0, s3 = 0;
-                int k = r + 1;
-                for (; k + 4 <= R; k += 4) {
-                    s0 -= A[k * LDA + r] * (Real)X(k);
-                    s1 -= A[(k + 1) * LDA + r] * (Real)X(k + 1);
-                    s2 -= A[(k + 2) * LDA + r] * (Real)X(k + 2);
-                    s3 -= A[(k + 3) * LDA + r] * (Real)X(k + 3);
-                }
-                for (; k < R; ++k) s0 -= A[k * LDA + r] * (Real)X(k);
-                const Real sr = (s0 + s1) + (s2 + s3);
-                X(r) = (double)(sr * invd[r]);
-            }
-#undef X
-        }
-    }
+    // ridge, Cholesky and the solve map in warp 0 alone (warp barriers
+    // only); the other warps wait at the next block barrier
+    if (tid < 32) warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
     __syncthreads();
     // Y = Yhat W (padding columns zero)
     for (uint32_t e = tid; e < total; e += nt) {
@@ -662,21 +597,29 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
 // std::mt19937_64, entries from std::normal_distribution<float>(0, 1),
 // row-major, padding zero.  Generated on the host, uploaded once.
 int init_factors_host(Plan& p, uint64_t seed) {
+    // one independent generator per mode: draw the modes on parallel host
+    // threads (large factors take seconds to draw serially)
+    std::vector<std::vector<float>> Y(p.N);
+    std::vector<std::thread> th;
+    for (int n = 0; n < p.N; ++n)
+        th.emplace_back([&, n]() {
+            uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
+            z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
+            z ^= z >> 27; z *= 0x94D049BB133111EBULL;
+            z ^= z >> 31;
+            std::mt19937_64 rng(z);
+            std::normal_distribution<float> g(0.0f, 1.0f);
+            Y[n].assign((size_t)p.dims[n] * p.Rp, 0.f);
+            for (uint32_t i = 0; i < p.dims[n]; ++i)
+                for (int r = 0; r < p.R; ++r) Y[n][(size_t)i * p.Rp + r] = g(rng);
+        });
+    for (auto& t : th) t.join();
     for (int n = 0; n < p.N; ++n) {
-        uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
-        z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
-        z ^= z >> 27; z *= 0x94D049BB133111EBULL;
-        z ^= z >> 31;
-        std::mt19937_64 rng(z);
-        std::normal_distribution<float> g(0.0f, 1.0f);
-        std::vector<float> Y((size_t)p.dims[n] * p.Rp, 0.f);
-        for (uint32_t i = 0; i < p.dims[n]; ++i)
-            for (int r = 0; r < p.R; ++r) Y[(size_t)i * p.Rp + r] = g(rng);
-        DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y.data(), Y.size() * sizeof(float),
+        DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y[n].data(), Y[n].size() * sizeof(float),
                                   cudaMemcpyHostToDevice, p.stream));
-        DGPU_CUDA(cudaStreamSynchronize(p.stream));
         p.yb_stale[n] = true;
     }
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
     return DGPU_OK;
 }
 

@@ -182,6 +182,8 @@ struct Plan {
     PartList     ident;                         // identity order over [0, nnz) (global)
     int          sms = 148;                     // SM count of the device
     int          part_fiber = 0;                // 1 while a fiber-sort partition runs (timing class)
+    int          rank_tile = 0;                 // MTTKRP columns per slab pass (0: tuned)
+    int          tile_for[kMaxModes] = {};      // tuned columns per slab pass, per mode
     // Widest LSD digit of shard sorts / remaps and of fiber sorts.  Above ~8
     // bits a pass writes runs of a few elements per bucket and window, which
     // costs more (uncoalesced stores, partial-sector DRAM writes) than a

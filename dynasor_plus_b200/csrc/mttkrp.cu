@@ -110,6 +110,8 @@ struct RunBatch {
 // shared slot array (prefetching the next chunk into registers), then walk
 // the chunk U nonzeros at a time: U x (N-1) float4 gathers in flight per
 // lane, products in registers, one vector atomic per finished row run.
+// Rp columns starting at the factor pointers are processed; ld is the row
+// stride (a rank tile of a wider factor has Rp < ld).
 // TN >= 0 pins the target mode at compile time (the reference's TGT
 // specialisation, src/dynasor_kernel.cpp:247-265), so only the N-1 gathered
 // rows occupy registers; TN = -1 takes the mode at run time.
@@ -117,7 +119,7 @@ template <int N, int G, int V, bool BF, int TN>
 __global__ void __launch_bounds__(kRunThreads, (RunBatch<N, V, BF>::kMinBlocks))
 k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ tiles,
                 const __grid_constant__ FacPtrs F, float* __restrict__ Yhat,
-                int n_rt, int w0_rt, int wl_rt, int Rp)
+                int n_rt, int w0_rt, int wl_rt, int Rp, int ld)
 {
     const int n = TN >= 0 ? TN : n_rt;
     const int w0 = TN >= 0 ? (TN == 0 ? 1 : 0) : w0_rt;
@@ -212,7 +214,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
                     for (int v = 0; v < V; ++v) {
                         const int c4 = gl + v * G;
                         float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, Rp, c4);
+                        if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
                         y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
                         y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
                     }
@@ -223,7 +225,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
                 if (e0 + u < cnt) {
                     if (row[u] != cur) {
                         if (cur != 0xffffffffu) {
-                            float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
+                            float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * ld);
 #pragma unroll
                             for (int v = 0; v < V; ++v) {
                                 const int c4 = gl + v * G;
@@ -258,7 +260,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
         __syncwarp();
     }
     if (cur != 0xffffffffu) {
-        float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * Rp);
+        float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * ld);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             const int c4 = gl + v * G;
@@ -433,18 +435,24 @@ int launch_priv(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntil
 
 template <int N, bool BF>
 int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
-                  const FacPtrs& F, int w0, int wl)
+                  const FacPtrs& F0, int w0, int wl, int c0, int cols)
 {
-    const int C4 = p.Rp / 4;
+    // columns [c0, c0 + cols) of every factor (a rank tile when cols < Rp)
+    const int C4 = cols / 4;
     const SlabPtrs sp = slab_in(in, p.N);
-    float* out = p.Yhat[n];
+    float* out = p.Yhat[n] + c0;
+    FacPtrs F = F0;
+    for (int w = 0; w < p.N; ++w) {
+        if (F.Y[w]) F.Y[w] += c0;
+        if (F.Yb[w]) F.Yb[w] += c0;
+    }
     // at least ~4 CTAs per SM: split tiles when the tensor has few of them
     const uint32_t want = 4u * (uint32_t)p.sms;
     const uint32_t split = ntiles >= want ? 1u : std::min(16u, (want + ntiles - 1) / std::max(1u, ntiles));
     const dim3 grid(ntiles, split);
 #define DGPU_RUNT(G, V, TN)                                                                      \
     k_mttkrp_rowrun<N, G, V, BF, TN><<<grid, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, \
-                                                                         w0, wl, p.Rp)
+                                                                         w0, wl, cols, p.Rp)
 #define DGPU_RUN(G, V) DGPU_RUNT(G, V, -1)
     // target-mode specialisations for the common 3- and 4-mode, Rp <= 128 shapes
 #define DGPU_RUN_TGT(G)                                                       \
@@ -467,7 +475,7 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
     else if (C4 <= 128) DGPU_RUN(32, 4);
     else if (C4 <= 256) DGPU_RUN(32, 8);
     else {
-        set_error("mttkrp: rank_padded %d exceeds the supported maximum 1024", p.Rp);
+        set_error("mttkrp: rank tile %d exceeds the supported maximum 1024", cols);
         return DGPU_ERR_ARG;
     }
 #undef DGPU_RUN_TGT
@@ -498,7 +506,53 @@ int launch_n(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
 {
     if (mttkrp_scheme(p, n) == DGPU_ACCUM_PRIVATE)
         return launch_priv<N, BF>(p, n, in, tiles, ntiles, F, w0, wl);
-    return launch_rowrun<N, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+    // Rank tiles: one pass over the slab per tile of `rt` columns.  Wide
+    // factors gather whole rows per nonzero, which spills the hot rows out
+    // of L1; narrower tiles re-read the slab but keep gathers cached.  The
+    // tile width is tuned once per mode: the first call times each candidate
+    // width (Rp, 128, 64, 32 that divide Rp) and keeps the fastest
+    // (DGPU_RANK_TILE fixes it instead).
+    auto run = [&](int rt) -> int {
+        for (int c0 = 0; c0 < p.Rp; c0 += rt) {
+            const int rc = launch_rowrun<N, BF>(p, n, in, tiles, ntiles, F, w0, wl, c0, rt);
+            if (rc != DGPU_OK) return rc;
+        }
+        return DGPU_OK;
+    };
+    if (p.rank_tile > 0 && p.rank_tile <= p.Rp && p.Rp % p.rank_tile == 0 && p.rank_tile % 16 == 0)
+        return run(p.rank_tile);
+    int& chosen = p.tile_for[n];
+    if (chosen == 0) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        DGPU_CUDA(cudaStreamIsCapturing(p.stream, &cs));
+        if (p.Rp <= 64 || cs != cudaStreamCaptureStatusNone || p.timing) return run(p.Rp);
+        const size_t yb = (size_t)p.dims[n] * p.Rp * sizeof(float);
+        cudaEvent_t a, b;
+        DGPU_CUDA(cudaEventCreate(&a));
+        DGPU_CUDA(cudaEventCreate(&b));
+        float best = 0.f;
+        int best_rt = p.Rp;
+        const int cands[4] = {p.Rp, 128, 64, 32};
+        for (int ci = 0; ci < 4; ++ci) {
+            const int rt = cands[ci];
+            bool seen = false;
+            for (int cj = 0; cj < ci; ++cj) seen = seen || cands[cj] == rt;
+            if (seen || rt > p.Rp || p.Rp % rt != 0) continue;
+            DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, yb, p.stream));
+            DGPU_CUDA(cudaEventRecord(a, p.stream));
+            DGPU_TRY(run(rt));
+            DGPU_CUDA(cudaEventRecord(b, p.stream));
+            DGPU_CUDA(cudaEventSynchronize(b));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (best == 0.f || ms < best) { best = ms; best_rt = rt; }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        chosen = best_rt;
+        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, yb, p.stream));
+    }
+    return run(chosen);
 }
 
 template <bool BF>

@@ -343,6 +343,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     // does not depend on them)
     if (const char* e = std::getenv("DGPU_SORT_DIGIT_BITS")) p.sort_digit_bits = std::atoi(e);
     if (const char* e = std::getenv("DGPU_FIBER_DIGIT_BITS")) p.fiber_digit_bits = std::atoi(e);
+    if (const char* e = std::getenv("DGPU_RANK_TILE")) p.rank_tile = std::atoi(e);
 
     // geometry
     for (int n = 0; n < p.N; ++n) {

@@ -212,6 +212,19 @@ void dgpu_cp_options_default(dgpu_cp_options* opt);
 int  dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt,
                 dgpu_cp_result* res, double* fit_history);
 
+/* K random-restart CP-ALS runs in one plan (no single reference function:
+ * the reference runs cpals, src/dynasor_cpals.cpp:120-396, once per seed).
+ * The plan's rank is restarts * Re (Re <= 64); restart k uses columns
+ * [k*Re, (k+1)*Re) of every factor, starts from the reference's N(0,1)
+ * initialisation with seed opt->seed + k (unless opt->use_init), and has its
+ * own fit and stop rule; a converged restart is frozen while the others
+ * continue.  One MTTKRP sweep serves all restarts.  res[restarts];
+ * fit_history (may be NULL) receives restarts x max_iters fits (row k =
+ * restart k, zero after its last iteration).  total_time_s is the batch's
+ * wall time; mttkrp_time_s and linalg_time_s are 0 (not split). */
+int  dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* opt,
+                           dgpu_cp_result* res, double* fit_history);
+
 /* ---- small dense kernels (replace la::*, include/dynasor_linalg.h:33-127),
  *      device pointers, FP32 row-major with leading dimension Rp --------- */
 int dgpu_la_gram(void* stream, const float* Y, uint64_t rows, int R, int Rp, float* G);
