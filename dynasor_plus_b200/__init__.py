@@ -26,7 +26,7 @@ import numpy as np
 from ._lib import (CpOptions, CpResult, Coo, DgpuError, PlanInfo, PlanOpts, TensorDesc, check,
                    lib, LIB_PATH)
 
-__all__ = ["Plan", "DgpuError", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
+__all__ = ["Plan", "DgpuError", "cpals_batch", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
            "spmttkrp_dynasor", "device_count", "LIB_PATH", "PINGPONG", "NCOPY"]
 
 PINGPONG = 0
@@ -367,3 +367,32 @@ def dump_factor_matrix_bin(path: str, Y, R: int):
     """DYFM factor dump (src/dynasor_io.cpp:1287-1348)."""
     Y = np.ascontiguousarray(Y, np.float32)
     check(lib().dgpu_dump_factor_bin(os.fsencode(path), Y.ctypes.data, Y.shape[0], int(R), Y.shape[1]))
+
+
+def cpals_batch(plans, max_iters=50, tol=1e-4, seed=42, ridge=1e-10, kernel="gs",
+                solve_fp64=True, use_init=False, graphs=True):
+    """Independent CP-ALS runs on several plans (one per tensor) whose
+    iterations after the first run as parallel device loops of one graph
+    launch.  Returns one result dict per plan (as Plan.cpals)."""
+    o = CpOptions()
+    lib().dgpu_cp_options_default(C.byref(o))
+    o.max_iters = int(max_iters)
+    o.tol = float(tol)
+    o.seed = int(seed)
+    o.ridge = float(ridge)
+    o.kernel = 1 if kernel in ("jacobi", "all-modes", "all_modes", "js") else 0
+    o.solve_fp64 = 1 if solve_fp64 else 0
+    o.use_init = 1 if use_init else 0
+    o.graphs = 1 if graphs else 0
+    K = len(plans)
+    hs = (C.c_void_p * K)(*[pl._h for pl in plans])
+    res = (CpResult * K)()
+    hist = np.zeros((K, max(1, int(max_iters))), np.float64)
+    check(lib().dgpu_cpals_batch(C.cast(hs, C.c_void_p), K, C.byref(o), C.cast(res, C.c_void_p),
+                                 hist.ctypes.data))
+    return [{"iters_done": r.iters_done, "final_fit": r.final_fit,
+             "final_residual": r.final_residual, "tensor_norm": r.tensor_norm,
+             "total_time_s": r.total_time_s, "mttkrp_time_s": r.mttkrp_time_s,
+             "linalg_time_s": r.linalg_time_s, "fit_history": hist[k, :r.iters_done].copy(),
+             "lambda": plans[k].lam()} for k, r in enumerate(res)]
+

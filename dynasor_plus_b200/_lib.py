@@ -101,6 +101,8 @@ _SIGS = {
     "dgpu_cpals": (C.c_int, [C.c_void_p, C.POINTER(CpOptions), C.POINTER(CpResult), C.c_void_p]),
     "dgpu_cpals_multistart": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CpOptions), C.c_void_p,
                                         C.c_void_p]),
+    "dgpu_cpals_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CpOptions), C.c_void_p,
+                                   C.c_void_p]),
     "dgpu_la_gram": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_void_p]),
     "dgpu_tensor_norm_sq": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "dgpu_model_values": (C.c_int, [C.c_void_p, C.c_void_p]),

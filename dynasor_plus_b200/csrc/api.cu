@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cstring>
 #include <new>
+#include <vector>
 
 namespace dgpu {
 int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o);
@@ -18,6 +19,8 @@ int mode_ncopy(Plan& p, int n);
 int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& r, double* fit_history);
 int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_result* res,
                          double* fit_history);
+int cpals_batch_run(Plan* const* plans, int count, const dgpu_cp_options& o,
+                    dgpu_cp_result* res, double* fit_history);
 }  // namespace dgpu
 
 using namespace dgpu;
@@ -385,6 +388,30 @@ int dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt, dgpu_cp_result* res,
     if (!opt || !res) { set_error("dgpu_cpals: null argument"); return DGPU_ERR_ARG; }
     if (opt->max_iters < 0) { set_error("dgpu_cpals: max_iters < 0"); return DGPU_ERR_ARG; }
     return cpals_run(*p, *opt, *res, fit_history);
+}
+
+int dgpu_cpals_batch(dgpu_plan* const* plans, int count, const dgpu_cp_options* opt,
+                     dgpu_cp_result* res, double* fit_history) {
+    if (!plans || !opt || !res || count < 1) {
+        set_error("dgpu_cpals_batch: null argument or count < 1");
+        return DGPU_ERR_ARG;
+    }
+    if (opt->max_iters < 0) { set_error("dgpu_cpals_batch: max_iters < 0"); return DGPU_ERR_ARG; }
+    std::vector<Plan*> ps(count);
+    for (int k = 0; k < count; ++k) {
+        ps[k] = reinterpret_cast<Plan*>(plans[k]);
+        if (!ps[k]) { set_error("dgpu_cpals_batch: plan %d is null", k); return DGPU_ERR_ARG; }
+        if (ps[k]->device != ps[0]->device) {
+            set_error("dgpu_cpals_batch: plans on different devices (%d, %d)", ps[0]->device,
+                      ps[k]->device);
+            return DGPU_ERR_ARG;
+        }
+        for (int j = 0; j < k; ++j)
+            if (ps[j] == ps[k]) { set_error("dgpu_cpals_batch: plan %d repeated", k); return DGPU_ERR_ARG; }
+    }
+    Plan* p = ps[0];
+    API_GUARD(p);
+    return cpals_batch_run(ps.data(), count, *opt, res, fit_history);
 }
 
 int dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* opt,

@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstdio>
 #include <random>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -641,48 +642,88 @@ int cp_tensor_norm(Plan& p, const float* vals, double* out) {
     return DGPU_OK;
 }
 
-int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fit_history) {
+// One CP-ALS run on a plan, in phases so that several runs can share one
+// graph launch (cpals_batch_run).  Iteration 0 runs eagerly (it allocates,
+// times the MTTKRP / update split and fixes tuned kernel choices); later
+// iterations run either as a device-side WHILE loop captured into a graph
+// (when an iteration leaves the live slab where it found it) or from the
+// host, replaying per-iteration graphs.
+struct CpSession {
     using clk = std::chrono::steady_clock;
-    res = dgpu_cp_result{};
+    Plan& p;
+    dgpu_cp_options o;
+    dgpu_cp_result& res;
+    double* fit_history;
     LaLayout L{};
-    DGPU_TRY(la_ensure(p, L));
-    if (!o.use_init) DGPU_TRY(init_factors_host(p, o.seed));
-    for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
-    double tn2 = 0;
-    const Slab& vs = (p.layout == DGPU_LAYOUT_NCOPY) ? p.slab[0] : p.slab[p.cur];
-    DGPU_TRY(cp_tensor_norm(p, vs.vals, &tn2));
-    res.tensor_norm = std::sqrt(tn2);
-    if (o.verbose)
-        std::printf("[cpals] modes=%d  rank=%d  padded=%d  nnz=%llu  ||T|| = %.6e  max_iters=%d  "
-                    "tol=%.1e  seed=%llu\n", p.N, p.R, p.Rp, (unsigned long long)p.nnz,
-                    res.tensor_norm, o.max_iters, o.tol, (unsigned long long)o.seed);
-
-    // Events: ev[0] iteration start, ev[1 + 2n] end of mode n's MTTKRP,
-    // ev[2 + 2n] end of its factor update (Jacobi: ev[1] ends the all-modes
-    // MTTKRP and ev[2 + 2n] each update).
-    const bool jacobi = (o.kernel == DGPU_CP_JACOBI);
-    const int nev = 2 * p.N + 2;
-    std::vector<cudaEvent_t> ev(nev, nullptr);
-    for (auto& e : ev) DGPU_CUDA(cudaEventCreate(&e));
-    double* fit_host = nullptr;              // pinned: the graph's D2H target
-    DGPU_CUDA(cudaMallocHost((void**)&fit_host, 4 * sizeof(double)));
-    struct Cleanup {
-        std::vector<cudaEvent_t>& ev; double* fh; cudaGraphExec_t* ex;
-        ~Cleanup() {
-            for (auto e : ev) if (e) cudaEventDestroy(e);
-            if (fh) cudaFreeHost(fh);
-            for (int k = 0; k < 2; ++k) if (ex[k]) cudaGraphExecDestroy(ex[k]);
-        }
-    };
+    double tn2 = 0.0;
+    bool jacobi = false;
+    std::vector<cudaEvent_t> ev;
+    double* fit_host = nullptr;              // pinned: the per-iteration graphs' D2H target
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int cur_after[2] = {0, 0};
-    Cleanup cleanup{ev, fit_host, exec};
+    double* st = nullptr;                    // device loop: [it, fit_prev] + fit/residual histories
+    size_t st_bytes = 0;
+    double fit_prev = 0.0;
+    int cur_start = 0;
+    int it = 0;                              // next iteration index
+    bool done = false;
+    bool graphs = false;
+    clk::time_point t_start;
+    // host plan state saved around a capture (a capture advances it without
+    // running the work)
+    int cur0 = 0, nm0 = 0;
+    bool stale0[kMaxModes] = {};
+
+    CpSession(Plan& pl, const dgpu_cp_options& op, dgpu_cp_result& r, double* fh)
+        : p(pl), o(op), res(r), fit_history(fh) {}
+    ~CpSession() {
+        for (auto e : ev) if (e) cudaEventDestroy(e);
+        if (fit_host) cudaFreeHost(fit_host);
+        for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
+        if (st) { dev_free(st); p.device_bytes -= st_bytes; }
+    }
+
+    int setup() {
+        res = dgpu_cp_result{};
+        DGPU_TRY(la_ensure(p, L));
+        if (!o.use_init) DGPU_TRY(init_factors_host(p, o.seed));
+        for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
+        const Slab& vs = (p.layout == DGPU_LAYOUT_NCOPY) ? p.slab[0] : p.slab[p.cur];
+        DGPU_TRY(cp_tensor_norm(p, vs.vals, &tn2));
+        res.tensor_norm = std::sqrt(tn2);
+        if (o.verbose)
+            std::printf("[cpals] modes=%d  rank=%d  padded=%d  nnz=%llu  ||T|| = %.6e  max_iters=%d  "
+                        "tol=%.1e  seed=%llu\n", p.N, p.R, p.Rp, (unsigned long long)p.nnz,
+                        res.tensor_norm, o.max_iters, o.tol, (unsigned long long)o.seed);
+        jacobi = (o.kernel == DGPU_CP_JACOBI);
+        // ev[0] iteration start, ev[1 + 2n] end of mode n's MTTKRP (Jacobi:
+        // ev[1] ends all MTTKRPs), ev[2 + 2n] end of mode n's factor update
+        ev.assign(2 * p.N + 2, nullptr);
+        for (auto& e : ev) DGPU_CUDA(cudaEventCreate(&e));
+        DGPU_CUDA(cudaMallocHost((void**)&fit_host, 4 * sizeof(double)));
+        graphs = o.graphs != 0 && !p.timing;
+        cur_start = p.cur;
+        done = o.max_iters <= 0;
+        t_start = clk::now();
+        return DGPU_OK;
+    }
+
+    void save_state() {
+        cur0 = p.cur;
+        nm0 = p.next_mode;
+        for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
+    }
+    void restore_state() {
+        p.cur = cur0;
+        p.next_mode = nm0;
+        for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
+    }
 
     // One iteration's work on p.stream.  kind 0: eager; 1: captured for
     // per-iteration replay (event records become graph event nodes); 2: the
     // body of the device-side loop (no events, no host copy; the loop
     // control kernel follows).
-    auto enqueue = [&](int kind) -> int {
+    int enqueue(int kind) {
         auto rec = [&](int i) -> cudaError_t {
             if (kind == 2) return cudaSuccess;
             return kind == 1 ? cudaEventRecordWithFlags(ev[i], p.stream, cudaEventRecordExternal)
@@ -716,124 +757,20 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
             DGPU_CUDA(cudaMemcpyAsync(fit_host, L.fitout, 4 * sizeof(double),
                                       cudaMemcpyDeviceToHost, p.stream));
         return DGPU_OK;
-    };
+    }
 
-    // Runs iterations first.. on the device; returns the number run in *done.
-    auto device_loop = [&](int first, double fit_before, int* done) -> int {
-        *done = 0;
-        const int left = o.max_iters - first;
-        if (left <= 0) return DGPU_OK;
-        double* st = nullptr;        // [it, fit_prev] + fit and residual histories
-        DGPU_TRY(dev_alloc(p, (void**)&st, (2 + 2 * (size_t)o.max_iters) * sizeof(double)));
-        struct Free { double* q; Plan& pl; size_t b;
-                      ~Free() { dev_free(q); pl.device_bytes -= b; } }
-            fr{st, p, (2 + 2 * (size_t)o.max_iters) * sizeof(double)};
-        const double init[2] = {(double)first, fit_before};
-        DGPU_CUDA(cudaMemcpyAsync(st, init, sizeof(init), cudaMemcpyHostToDevice, p.stream));
-        DGPU_CUDA(cudaStreamSynchronize(p.stream));
-        cudaGraph_t outer = nullptr;
-        cudaGraphExec_t gx = nullptr;
-        struct G { cudaGraph_t& g; cudaGraphExec_t& x;
-                   ~G() { if (x) cudaGraphExecDestroy(x); if (g) cudaGraphDestroy(g); } } gg{outer, gx};
-        DGPU_CUDA(cudaGraphCreate(&outer, 0));
-        cudaGraphConditionalHandle h;
-        DGPU_CUDA(cudaGraphConditionalHandleCreate(&h, outer, 1, cudaGraphCondAssignDefault));
-        cudaGraphNodeParams np{};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = h;
-        np.conditional.type = cudaGraphCondTypeWhile;
-        np.conditional.size = 1;
-        cudaGraphNode_t node;
-        DGPU_CUDA(cudaGraphAddNode(&node, outer, nullptr, 0, &np));
-        cudaGraph_t body = np.conditional.phGraph_out[0];
-        const int cur0 = p.cur, nm0 = p.next_mode;
-        bool stale0[kMaxModes];
-        for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
-        auto restore = [&]() {
-            p.cur = cur0;
-            p.next_mode = nm0;
-            for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
-        };
-        if (cudaStreamBeginCaptureToGraph(p.stream, body, nullptr, nullptr, 0,
-                                          cudaStreamCaptureModeRelaxed) != cudaSuccess) {
-            cudaGetLastError();
-            set_error("cpals: device loop capture not available; iterating from the host");
-            return DGPU_ERR_CUDA;
-        }
-        int rc = enqueue(2);
-        if (rc == DGPU_OK) {
-            k_loop_ctl<<<1, 32, 0, p.stream>>>(h, L.fitout, st, st + 2, st + 2 + o.max_iters,
-                                               o.tol, o.max_iters);
-            if (cudaGetLastError() != cudaSuccess) rc = DGPU_ERR_CUDA;
-        }
-        cudaGraph_t cap = nullptr;
-        const cudaError_t ec = cudaStreamEndCapture(p.stream, &cap);
-        if (rc != DGPU_OK || ec != cudaSuccess || cudaGraphInstantiate(&gx, outer, 0) != cudaSuccess) {
-            cudaGetLastError();
-            restore();
-            if (rc != DGPU_OK && rc != DGPU_ERR_CUDA) return rc;
-            set_error("cpals: device loop graph not available; iterating from the host");
-            return DGPU_ERR_CUDA;
-        }
-        DGPU_CUDA(cudaEventRecord(ev[0], p.stream));
-        DGPU_CUDA(cudaGraphLaunch(gx, p.stream));
-        DGPU_CUDA(cudaEventRecord(ev[1], p.stream));
-        DGPU_CUDA(cudaStreamSynchronize(p.stream));
-        std::vector<double> hs(2 + 2 * (size_t)o.max_iters);
-        DGPU_CUDA(cudaMemcpy(hs.data(), st, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        const int last = (int)hs[0];           // iterations completed so far
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev[0], ev[1]);
-        // the loop's device time, split between MTTKRP and the factor
-        // updates in the proportion measured on the first (eager) iteration
-        const double tot = res.mttkrp_time_s + res.linalg_time_s;
-        const double fm = tot > 0 ? res.mttkrp_time_s / tot : 0.5;
-        res.mttkrp_time_s += fm * ms * 1e-3;
-        res.linalg_time_s += (1.0 - fm) * ms * 1e-3;
-        for (int i = first; i < last; ++i) {
-            if (fit_history) fit_history[i] = hs[2 + i];
-            res.final_fit = hs[2 + i];
-            res.final_residual = hs[2 + o.max_iters + i];
-        }
-        res.iters_done = last;
-        *done = last - first;
-        return DGPU_OK;
-    };
-
-    // Graph replay: the launches of an iteration depend only on which slab
-    // holds the mode-0 order when it starts (PingPong), so at most two graphs
-    // are captured; host-side plan state is advanced as the capture left it.
-    bool graphs = o.graphs != 0 && !p.timing;
-    double fit_prev = 0.0;
-    const auto t_start = clk::now();
-    const int cur_start = p.cur;
-    for (int it = 0; it < o.max_iters; ++it) {
+    // One host-driven iteration: eager, or (after the first) a replay of the
+    // per-iteration graph keyed by the live slab (PingPong alternates slabs,
+    // so at most two graphs), then the fit bookkeeping and the stop rule.
+    int step_host() {
         const auto t_it = clk::now();
         const int key = (p.layout == DGPU_LAYOUT_NCOPY) ? 0 : (p.cur & 1);
-        // After the first (eager) iteration, when an iteration leaves the
-        // live slab where it found it, the remaining iterations run as one
-        // graph launch: a device-side WHILE loop whose body is one iteration
-        // plus a control kernel that records the fit and applies the
-        // reference's stop rule (no host round trip per iteration).
-        if (graphs && it == 1 && !o.verbose &&
-            (p.layout == DGPU_LAYOUT_NCOPY || p.cur == cur_start)) {
-            int done = 0;
-            const int rc = device_loop(it, fit_prev, &done);
-            if (rc == DGPU_OK && done > 0) break;
-            if (rc != DGPU_OK && rc != DGPU_ERR_CUDA) return rc;
-            graphs = rc == DGPU_OK;      // capture unsupported: continue eagerly
-        }
         if (graphs && it > 0 && exec[key]) {
             DGPU_CUDA(cudaGraphLaunch(exec[key], p.stream));
             p.cur = cur_after[key];
             p.next_mode = 0;
         } else if (graphs && it > 0) {
-            // capturing advances the host-side plan state (live slab, next
-            // mode, BF16 mirror flags) without running the work; keep the
-            // state to restore it if the capture cannot be used
-            const int cur0 = p.cur, nm0 = p.next_mode;
-            bool stale0[kMaxModes];
-            for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
+            save_state();
             cudaGraph_t g = nullptr;
             cudaError_t ec = cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeRelaxed);
             int rc = DGPU_OK;
@@ -854,9 +791,7 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
                 cudaGetLastError();
                 exec[key] = nullptr;
                 graphs = false;
-                p.cur = cur0;
-                p.next_mode = nm0;
-                for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
+                restore_state();
                 DGPU_TRY(enqueue(0));
             }
         } else {
@@ -871,33 +806,185 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
             mt_ms += a;
             la_ms += b;
         }
-        const double* fo = fit_host;
-        const double fit = fo[2];
+        const double fit = fit_host[2];
         res.mttkrp_time_s += mt_ms * 1e-3;
         res.linalg_time_s += la_ms * 1e-3;
         if (fit_history) fit_history[it] = fit;
         res.final_fit = fit;
-        res.final_residual = fo[3];
+        res.final_residual = fit_host[3];
         res.iters_done = it + 1;
         const double iter_s = std::chrono::duration<double>(clk::now() - t_it).count();
         if (o.verbose)
             std::printf("[cpals] iter %3d  fit = %.6f  dfit = %.2e  resid = %.3e  iter = %.3f s\n",
-                        it, fit, it == 0 ? 0.0 : std::fabs(fit - fit_prev), fo[3], iter_s);
+                        it, fit, it == 0 ? 0.0 : std::fabs(fit - fit_prev), fit_host[3], iter_s);
         if (it > 0 && std::fabs(fit - fit_prev) < o.tol) {
             if (o.verbose)
                 std::printf("[cpals] converged after %d iterations (|dfit|=%.2e < %.1e)\n", it + 1,
                             std::fabs(fit - fit_prev), o.tol);
-            break;
+            done = true;
         }
         fit_prev = fit;
+        ++it;
+        if (it >= o.max_iters) done = true;
+        return DGPU_OK;
     }
-    res.total_time_s = std::chrono::duration<double>(clk::now() - t_start).count();
-    if (o.verbose)
-        std::printf("[cpals] done  iters=%d  final_fit=%.6f  resid=%.3e\n"
-                    "[cpals] total = %.3f s   spMTTKRP = %.3f s (%.1f%%)   linalg  = %.3f s (%.1f%%)\n",
-                    res.iters_done, res.final_fit, res.final_residual, res.total_time_s,
-                    res.mttkrp_time_s, 100.0 * res.mttkrp_time_s / std::max(res.total_time_s, 1e-30),
-                    res.linalg_time_s, 100.0 * res.linalg_time_s / std::max(res.total_time_s, 1e-30));
+
+    // The remaining iterations can run as a device-side loop.
+    bool loop_eligible() const {
+        return graphs && !done && it == 1 && !o.verbose &&
+               (p.layout == DGPU_LAYOUT_NCOPY || p.cur == cur_start);
+    }
+
+    // Captures one iteration + the loop control into `body` (the WHILE
+    // node's graph).  DGPU_ERR_CUDA: capture not possible (state restored).
+    int capture_body(cudaGraph_t body, cudaGraphConditionalHandle h) {
+        if (!st) {
+            st_bytes = (2 + 2 * (size_t)o.max_iters) * sizeof(double);
+            DGPU_TRY(dev_alloc(p, (void**)&st, st_bytes));
+        }
+        const double init[2] = {(double)it, fit_prev};
+        DGPU_CUDA(cudaMemcpyAsync(st, init, sizeof(init), cudaMemcpyHostToDevice, p.stream));
+        DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        save_state();
+        if (cudaStreamBeginCaptureToGraph(p.stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cpals: device loop capture not available; iterating from the host");
+            return DGPU_ERR_CUDA;
+        }
+        int rc = enqueue(2);
+        if (rc == DGPU_OK) {
+            k_loop_ctl<<<1, 32, 0, p.stream>>>(h, L.fitout, st, st + 2, st + 2 + o.max_iters,
+                                               o.tol, o.max_iters);
+            if (cudaGetLastError() != cudaSuccess) rc = DGPU_ERR_CUDA;
+        }
+        cudaGraph_t cap = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(p.stream, &cap);
+        if (rc != DGPU_OK || ec != cudaSuccess) {
+            cudaGetLastError();
+            restore_state();
+            if (rc != DGPU_OK && rc != DGPU_ERR_CUDA) return rc;
+            set_error("cpals: device loop graph not available; iterating from the host");
+            return DGPU_ERR_CUDA;
+        }
+        return DGPU_OK;
+    }
+
+    // After the loop graph ran: iterations, fits and the time split (the
+    // loop's device time `ms`, divided between MTTKRP and the factor updates
+    // in the proportion measured on the eager first iteration).
+    int finish_loop(float ms) {
+        std::vector<double> hs(2 + 2 * (size_t)o.max_iters);
+        DGPU_CUDA(cudaMemcpy(hs.data(), st, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        const int last = (int)hs[0];
+        const double tot = res.mttkrp_time_s + res.linalg_time_s;
+        const double fm = tot > 0 ? res.mttkrp_time_s / tot : 0.5;
+        res.mttkrp_time_s += fm * ms * 1e-3;
+        res.linalg_time_s += (1.0 - fm) * ms * 1e-3;
+        for (int i = it; i < last; ++i) {
+            if (fit_history) fit_history[i] = hs[2 + i];
+            res.final_fit = hs[2 + i];
+            res.final_residual = hs[2 + o.max_iters + i];
+        }
+        res.iters_done = last;
+        it = last;
+        done = true;
+        return DGPU_OK;
+    }
+
+    void finish() {
+        res.total_time_s = std::chrono::duration<double>(clk::now() - t_start).count();
+        if (o.verbose)
+            std::printf("[cpals] done  iters=%d  final_fit=%.6f  resid=%.3e\n"
+                        "[cpals] total = %.3f s   spMTTKRP = %.3f s (%.1f%%)   linalg  = %.3f s (%.1f%%)\n",
+                        res.iters_done, res.final_fit, res.final_residual, res.total_time_s,
+                        res.mttkrp_time_s, 100.0 * res.mttkrp_time_s / std::max(res.total_time_s, 1e-30),
+                        res.linalg_time_s, 100.0 * res.linalg_time_s / std::max(res.total_time_s, 1e-30));
+    }
+};
+
+// Runs the device loops of `ss` (all eligible) as parallel WHILE nodes of one
+// graph, launched once on `launch`.  Sessions whose capture is not possible
+// are left to iterate from the host.
+int run_loops(std::vector<CpSession*>& ss, cudaStream_t launch) {
+    cudaGraph_t outer = nullptr;
+    cudaGraphExec_t gx = nullptr;
+    struct G { cudaGraph_t& g; cudaGraphExec_t& x;
+               ~G() { if (x) cudaGraphExecDestroy(x); if (g) cudaGraphDestroy(g); } } gg{outer, gx};
+    DGPU_CUDA(cudaGraphCreate(&outer, 0));
+    std::vector<CpSession*> in;
+    for (CpSession* s : ss) {
+        cudaGraphConditionalHandle h;
+        DGPU_CUDA(cudaGraphConditionalHandleCreate(&h, outer, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        DGPU_CUDA(cudaGraphAddNode(&node, outer, nullptr, 0, &np));
+        const int rc = s->capture_body(np.conditional.phGraph_out[0], h);
+        if (rc == DGPU_OK) { in.push_back(s); continue; }
+        if (rc != DGPU_ERR_CUDA) return rc;
+        s->graphs = false;                       // iterate this one from the host
+        DGPU_CUDA(cudaGraphDestroyNode(node));
+    }
+    if (in.empty()) return DGPU_OK;
+    if (cudaGraphInstantiate(&gx, outer, 0) != cudaSuccess) {
+        cudaGetLastError();
+        for (CpSession* s : in) { s->restore_state(); s->graphs = false; }
+        return DGPU_OK;
+    }
+    cudaEvent_t a, b;
+    DGPU_CUDA(cudaEventCreate(&a));
+    DGPU_CUDA(cudaEventCreate(&b));
+    DGPU_CUDA(cudaEventRecord(a, launch));
+    DGPU_CUDA(cudaGraphLaunch(gx, launch));
+    DGPU_CUDA(cudaEventRecord(b, launch));
+    DGPU_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    for (CpSession* s : in) DGPU_TRY(s->finish_loop(ms));
+    return DGPU_OK;
+}
+
+int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fit_history) {
+    CpSession s(p, o, res, fit_history);
+    DGPU_TRY(s.setup());
+    if (!s.done) DGPU_TRY(s.step_host());
+    if (s.loop_eligible()) {
+        std::vector<CpSession*> one{&s};
+        DGPU_TRY(run_loops(one, p.stream));
+    }
+    while (!s.done) DGPU_TRY(s.step_host());
+    s.finish();
+    return DGPU_OK;
+}
+
+// Independent CP-ALS runs on several plans (one per tensor) whose remaining
+// iterations run as parallel device loops of one graph launch.
+int cpals_batch_run(Plan* const* plans, int count, const dgpu_cp_options& o,
+                    dgpu_cp_result* res, double* fit_history) {
+    std::vector<std::unique_ptr<CpSession>> ss;
+    for (int k = 0; k < count; ++k) {
+        ss.emplace_back(new CpSession(*plans[k], o, res[k],
+                                      fit_history ? fit_history + (size_t)k * std::max(1, o.max_iters)
+                                                  : nullptr));
+        CpSession& s = *ss.back();
+        DGPU_CUDA(cudaSetDevice(plans[k]->device));
+        DGPU_TRY(s.setup());
+        if (!s.done) DGPU_TRY(s.step_host());
+    }
+    std::vector<CpSession*> loop;
+    for (auto& s : ss)
+        if (s->loop_eligible()) loop.push_back(s.get());
+    if (!loop.empty()) DGPU_TRY(run_loops(loop, plans[0]->stream));
+    for (auto& s : ss) {
+        while (!s->done) DGPU_TRY(s->step_host());
+        s->finish();
+    }
     return DGPU_OK;
 }
 

@@ -224,6 +224,14 @@ int  dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt,
  * wall time; mttkrp_time_s and linalg_time_s are 0 (not split). */
 int  dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* opt,
                            dgpu_cp_result* res, double* fit_history);
+/* Independent CP-ALS runs on `count` plans (one per tensor, same device),
+ * each as dgpu_cpals would run it; after every plan's first iteration the
+ * remaining iterations of all plans run as parallel device-side loops of
+ * one CUDA graph launch (no reference counterpart: the reference decomposes
+ * one tensor per process).  res[count]; fit_history (may be NULL) receives
+ * count x max_iters fits, row k for plans[k]. */
+int  dgpu_cpals_batch(dgpu_plan* const* plans, int count, const dgpu_cp_options* opt,
+                      dgpu_cp_result* res, double* fit_history);
 
 /* ---- small dense kernels (replace la::*, include/dynasor_linalg.h:33-127),
  *      device pointers, FP32 row-major with leading dimension Rp --------- */
