@@ -94,13 +94,16 @@ constexpr int kRunWarps = kRunThreads / 32;
 
 // Nonzeros whose gathers a lane group keeps in flight together (U) and the
 // CTAs per SM the kernel is compiled for.  The kernel is bound by gather
-// latency, so occupancy (64 registers, 4 CTAs of 256 threads) pays more than
-// a deeper batch; BF16 rows take half the registers, so BF16 batches deeper.
+// latency, so occupancy (40-64 registers, 4-6 CTAs of 256 threads) pays more
+// than a deeper batch; BF16 rows take half the registers, so BF16 batches
+// deeper.
 template <int N, int V, bool BF>
 struct RunBatch {
     static constexpr int kWork = (N - 1) * V;
-    static constexpr int U = kWork <= 2 ? (BF ? 4 : 2) : (kWork <= 4 ? 2 : 1);
-    static constexpr int kMinBlocks = N <= 4 ? 4 : 2;
+    // measured on the 3-mode rank-32 Zipf tensor (MTTKRP ms per sweep):
+    // 4 CTAs/U=2 3.68, 5/1 3.60, 6/1 3.45, 8/1 3.66 (spills), 4/1 4.03
+    static constexpr int U = kWork <= 2 ? (BF ? 4 : 1) : (kWork <= 4 ? 2 : 1);
+    static constexpr int kMinBlocks = (kWork <= 2 && !BF) ? 6 : (N <= 4 ? 4 : 2);
 };
 
 // One CTA per tile.  Warp w owns the w-th contiguous slice of the tile and

@@ -63,35 +63,56 @@ __device__ __forceinline__ uint32_t part_key(uint32_t v, int shift, uint32_t mas
     return (v >> shift) & mask;
 }
 
+// One CTA per chunk.  With `copies` > 1 every warp group counts into its
+// own copy of the histogram (fewer shared-atomic collisions on skewed keys:
+// hot rows of a Zipf mode land in few buckets); the copies are summed at the
+// end.
 __global__ void __launch_bounds__(kHistThreads)
 k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles,
              const Chunk* __restrict__ chunks, int shift, uint32_t mask, uint32_t nb,
-             uint32_t* __restrict__ cnt)
+             int copies, uint32_t* __restrict__ cnt)
 {
-    extern __shared__ uint32_t h[];
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) h[b] = 0;
+    extern __shared__ uint32_t h[];                 // [copies][nb]
+    for (uint32_t b = threadIdx.x; b < nb * copies; b += blockDim.x) h[b] = 0;
     __syncthreads();
+    uint32_t* hc = h + (size_t)((threadIdx.x >> 5) % copies) * nb;
     const Chunk c = chunks[blockIdx.x];
     for (uint32_t t = c.tile_begin; t < c.tile_end; ++t) {
         const Tile tl = tiles[t];
         const uint32_t* k = keycol + tl.begin;
-        // four independent loads in flight per thread
-        const uint32_t rounds = (tl.count + 4 * blockDim.x - 1) / (4 * blockDim.x);
-        for (uint32_t r = 0; r < rounds; ++r) {
-            uint32_t kk[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t j = (r * 4 + q) * blockDim.x + threadIdx.x;
-                kk[q] = j < tl.count ? part_key(__ldg(k + j), shift, mask) : 0xffffffffu;
+        // scalar head up to a 16-byte boundary (the column starts 256-byte
+        // aligned), 16-byte loads two at a time (8 keys per thread in
+        // flight), scalar tail
+        const uint32_t head = min(tl.count, (4u - (tl.begin & 3u)) & 3u);
+        for (uint32_t j = threadIdx.x; j < head; j += blockDim.x)
+            atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
+        const uint32_t n4 = (tl.count - head) >> 2;
+        const uint4* k4 = reinterpret_cast<const uint4*>(k + head);
+        for (uint32_t i = threadIdx.x; i < n4; i += 2 * blockDim.x) {
+            const uint4 a = __ldg(k4 + i);
+            const bool two = i + blockDim.x < n4;
+            const uint4 b = two ? __ldg(k4 + i + blockDim.x) : make_uint4(0u, 0u, 0u, 0u);
+            atomicAdd(&hc[part_key(a.x, shift, mask)], 1u);
+            atomicAdd(&hc[part_key(a.y, shift, mask)], 1u);
+            atomicAdd(&hc[part_key(a.z, shift, mask)], 1u);
+            atomicAdd(&hc[part_key(a.w, shift, mask)], 1u);
+            if (two) {
+                atomicAdd(&hc[part_key(b.x, shift, mask)], 1u);
+                atomicAdd(&hc[part_key(b.y, shift, mask)], 1u);
+                atomicAdd(&hc[part_key(b.z, shift, mask)], 1u);
+                atomicAdd(&hc[part_key(b.w, shift, mask)], 1u);
             }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (kk[q] != 0xffffffffu) atomicAdd(&h[kk[q]], 1u);
         }
+        for (uint32_t j = head + 4 * n4 + threadIdx.x; j < tl.count; j += blockDim.x)
+            atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
     }
     __syncthreads();
     uint32_t* out = cnt + (size_t)blockIdx.x * nb;
-    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) out[b] = h[b];
+    for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) {
+        uint32_t v = 0;
+        for (int q = 0; q < copies; ++q) v += h[(size_t)q * nb + b];
+        out[b] = v;
+    }
 }
 
 // grid (segments, ceil(nb/256)); thread = bucket.
@@ -632,8 +653,11 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
     {
         LaunchTimer t(p, p.part_fiber ? KK_FIB_HIST : KK_PART_HIST,
                       elem * 4.0 + (double)L.nchunks * nb * 4.0);
-        k_chunk_hist<<<L.nchunks, kHistThreads, nb * sizeof(uint32_t), p.stream>>>(
-            in.idx[key_mode], L.tiles, L.chunks, key_shift, key_mask, nb, p.part_cnt);
+        // one histogram copy per warp while 32 copies fit in 48 KB
+        const int copies = (int)std::max<uint32_t>(1u, std::min<uint32_t>(kHistThreads / 32,
+                                                                          12288u / nb));
+        k_chunk_hist<<<L.nchunks, kHistThreads, (size_t)copies * nb * sizeof(uint32_t), p.stream>>>(
+            in.idx[key_mode], L.tiles, L.chunks, key_shift, key_mask, nb, copies, p.part_cnt);
         DGPU_CUDA(cudaGetLastError());
     }
     {
