@@ -312,26 +312,72 @@ int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y, float* const*
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
     if (!Y || !Yhat) { set_error("dgpu_mttkrp_sweep_host: null"); return DGPU_ERR_ARG; }
-    for (int n = 0; n < p->N; ++n) DGPU_TRY(dgpu_upload_factor(plan, n, Y[n]));
-    cudaEvent_t e0, e1;
+    for (int n = 0; n < p->N; ++n)
+        if (!Y[n] || !Yhat[n]) { set_error("dgpu_mttkrp_sweep_host: null factor %d", n); return DGPU_ERR_ARG; }
+    if (p->next_mode != 0 && p->layout == DGPU_LAYOUT_PINGPONG) {
+        set_error("dgpu_mttkrp_sweep_host: the slab is ordered for mode %d, a sweep starts at 0",
+                  p->next_mode);
+        return DGPU_ERR_ORDER;
+    }
+    // Transfers overlap the mode passes on a second stream: the factors mode 0
+    // gathers go first, Y[0] (first needed by mode 1) streams in while mode 0
+    // runs, and each Yhat[n] streams out while the later modes run.  With
+    // pinned host buffers only the first uploads and the last download are
+    // exposed.
+    if (!p->copy_stream) DGPU_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    const int N = p->N;
+    std::vector<cudaEvent_t> up(N, nullptr), done(N, nullptr);
+    cudaEvent_t e0 = nullptr, e1 = nullptr, start = nullptr;
+    struct Ev {
+        std::vector<cudaEvent_t>& a; std::vector<cudaEvent_t>& b; cudaEvent_t* c[3];
+        ~Ev() {
+            for (auto e : a) if (e) cudaEventDestroy(e);
+            for (auto e : b) if (e) cudaEventDestroy(e);
+            for (auto e : c) if (*e) cudaEventDestroy(*e);
+        }
+    } evg{up, done, {&e0, &e1, &start}};
+    for (int n = 0; n < N; ++n) {
+        DGPU_CUDA(cudaEventCreateWithFlags(&up[n], cudaEventDisableTiming));
+        DGPU_CUDA(cudaEventCreateWithFlags(&done[n], cudaEventDisableTiming));
+    }
     DGPU_CUDA(cudaEventCreate(&e0));
     DGPU_CUDA(cudaEventCreate(&e1));
-    DGPU_CUDA(cudaEventRecord(e0, p->stream));
-    int rc = dgpu_mttkrp_sweep(plan);
-    if (rc == DGPU_OK) {
-        DGPU_CUDA(cudaEventRecord(e1, p->stream));
-        for (int n = 0; n < p->N && rc == DGPU_OK; ++n)
-            rc = (cudaMemcpyAsync(Yhat[n], p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
-                                  cudaMemcpyDeviceToHost, p->stream) == cudaSuccess)
-                     ? DGPU_OK : DGPU_ERR_CUDA;
-        const int rs = sync_checked(*p);
-        if (rc == DGPU_OK) rc = rs;
+    DGPU_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    // the copy stream starts after everything already queued on the plan stream
+    DGPU_CUDA(cudaEventRecord(start, p->stream));
+    DGPU_CUDA(cudaStreamWaitEvent(p->copy_stream, start, 0));
+    for (int k = 1; k <= N; ++k) {
+        const int w = k % N;                       // 1, 2, ..., N-1, then 0
+        DGPU_CUDA(cudaMemcpyAsync(p->Y[w], Y[w], (size_t)p->dims[w] * p->Rp * sizeof(float),
+                                  cudaMemcpyHostToDevice, p->copy_stream));
+        DGPU_CUDA(cudaEventRecord(up[w], p->copy_stream));
+        p->yb_stale[w] = true;
+    }
+    int rc = DGPU_OK;
+    for (int n = 0; n < N && rc == DGPU_OK; ++n) {
+        for (int w = 0; w < N; ++w)
+            if (w != n) DGPU_CUDA(cudaStreamWaitEvent(p->stream, up[w], 0));
+        if (n == 0) DGPU_CUDA(cudaEventRecord(e0, p->stream));
+        rc = (p->layout == DGPU_LAYOUT_NCOPY) ? mode_ncopy(*p, n) : mode_pingpong(*p, n);
+        if (rc != DGPU_OK) break;
+        DGPU_CUDA(cudaEventRecord(done[n], p->stream));
+        DGPU_CUDA(cudaStreamWaitEvent(p->copy_stream, done[n], 0));
+        DGPU_CUDA(cudaMemcpyAsync(Yhat[n], p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
+                                  cudaMemcpyDeviceToHost, p->copy_stream));
+    }
+    if (rc == DGPU_OK) DGPU_CUDA(cudaEventRecord(e1, p->stream));
+    const cudaError_t ec = cudaStreamSynchronize(p->copy_stream);
+    const int rs = sync_checked(*p);
+    if (rc == DGPU_OK && ec != cudaSuccess) {
+        set_error("dgpu_mttkrp_sweep_host: %s", cudaGetErrorString(ec));
+        rc = DGPU_ERR_CUDA;
+    }
+    if (rc == DGPU_OK) rc = rs;
+    if (rc == DGPU_OK && secs) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (secs) *secs = ms * 1e-3;
+        *secs = ms * 1e-3;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     return rc;
 }
 

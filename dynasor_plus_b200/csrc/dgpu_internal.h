@@ -173,6 +173,7 @@ struct Plan {
     // ---- device state -------------------------------------------------
     cudaStream_t stream = nullptr;
     bool         own_stream = false;
+    cudaStream_t copy_stream = nullptr;         // host transfers overlapping the sweep
     Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for

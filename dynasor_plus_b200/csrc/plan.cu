@@ -181,6 +181,7 @@ Plan::~Plan() {
     dev_free(lambda);
     dev_free(la_work);
     dev_free(la_f32);
+    if (copy_stream) { cudaStreamSynchronize(copy_stream); cudaStreamDestroy(copy_stream); }
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 

@@ -196,7 +196,11 @@ int dgpu_mttkrp_sweep(dgpu_plan* plan);
  * spmttkrp_all_modes_dynasor, src/dynasor.cpp:592-817). */
 int dgpu_mttkrp_all_modes(dgpu_plan* plan);
 /* Host-buffer convenience: upload Y[0..N-1], one sweep, download
- * Yhat[0..N-1]; returns the device seconds of the sweep in *secs. */
+ * Yhat[0..N-1] (spmttkrp_dynasor on host factor matrices).  Transfers run
+ * on a second stream overlapping the mode passes (Y[0] while mode 0 runs,
+ * Yhat[n] while the later modes run); pinned host buffers make that
+ * overlap real.  Returns when all copies are done; *secs = device seconds
+ * of the mode passes. */
 int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y,
                            float* const* Yhat, double* secs);
 
