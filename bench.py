@@ -55,7 +55,7 @@ METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 NCU_DRAM_BYTES_PER_NNZ = {
     "part_scatter": 29.49,     # k_chunk_scatter, all launches averaged
     "fiber_scatter": 29.49,
-    "mttkrp": 35.36,           # k_mttkrp_rowrun, 3 modes averaged
+    "mttkrp": 38.55,           # k_mttkrp_rowrun, 3 modes averaged
 }
 
 
@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--draws", type=int, default=DRAWS)
     ap.add_argument("--rank", type=int, default=RANK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ncopy", action="store_true", help="skip the NCopy-layout line")
     ap.add_argument("--cpu-sample", type=int, default=8_000_000,
                     help="nonzeros in the CPU-baseline sample")
     ap.add_argument("--cpals-iters", type=int, default=5)
@@ -262,6 +263,12 @@ def run_reference_arm(args):
                          "sample": f"random {nnz} of {len(vals)} nonzeros, same dims"},
         "e2e": {"value": val, "unit": "GNNZ/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        # the reference's fastest layout (NCopy: no remap) on the same sample
+        tn = statistics.median(reference_sweeps(d2, v2, i2, cores, args.rank, 1, 3, layout="ncopy"))
+        out["ncopy"] = {"value": nnz / tn / 1e9, "unit": "GNNZ/s", "ms_per_step": tn * 1e3}
+    except Exception as ex:  # reported, never required
+        out["ncopy"] = {"error": str(ex)[:200]}
     try:
         out["cpals_small"] = {"workload": "200x200x200, 100k nnz, rank 16, GS, tol 1e-4",
                               "threads": cores, **cpals_small_reference(cores)}
@@ -452,6 +459,28 @@ def main():
             out["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
 
     plan.close()
+
+    # the same metric on the NCopy layout (one pre-sorted copy per mode, no
+    # remap): the reference planner's choice when memory allows
+    if rank == 0 and args.layout == "pingpong" and not args.no_ncopy:
+        nc = d.Plan(dims, vals, idx, threads=args.threads, rank=args.rank, layout="ncopy",
+                    fiber=bool(args.fiber), precision=args.precision, device=local)
+        nc.set_stream(stream)
+        for n in range(N):
+            nc.set_factor(n, Y[n])
+        for _ in range(args.warmup):
+            nc.sweep()
+        nc.sync()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(args.steps):
+            nc.sweep()
+        c1.record(stream)
+        c1.synchronize()
+        nms = c0.elapsed_time(c1) / args.steps
+        out["ncopy"] = {"value": nnz / (nms * 1e-3) / 1e9, "unit": "GNNZ/s", "ms_per_step": nms}
+        nc.close()
     if rank == 0:
         s = json.dumps(out)
         print(s)
