@@ -122,7 +122,7 @@ template <int N, int G, int V, bool BF, int TN>
 __global__ void __launch_bounds__(kRunThreads, (RunBatch<N, V, BF>::kMinBlocks))
 k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ tiles,
                 const __grid_constant__ FacPtrs F, float* __restrict__ Yhat,
-                int n_rt, int w0_rt, int wl_rt, int Rp, int ld)
+                int n_rt, int w0_rt, int wl_rt, int Rp, int ld, int rows_contiguous)
 {
     const int n = TN >= 0 ? TN : n_rt;
     const int w0 = TN >= 0 ? (TN == 0 ? 1 : 0) : w0_rt;
@@ -165,6 +165,7 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[v][q] = 0.f;
     uint32_t cur = 0xffffffffu;
+    bool first_run = true;                 // the run at the start of this group's slice
 
     // prefetch registers for one chunk
     uint32_t pf[LPE][SW];
@@ -229,14 +230,22 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
                     if (row[u] != cur) {
                         if (cur != 0xffffffffu) {
                             float4* out = reinterpret_cast<float4*>(Yhat + (size_t)cur * ld);
+                            // a run that neither starts nor ends this group's
+                            // slice holds every nonzero of its row when rows
+                            // are contiguous (fiber-sorted): store, no atomic
+                            const bool own = rows_contiguous && !first_run;
 #pragma unroll
                             for (int v = 0; v < V; ++v) {
                                 const int c4 = gl + v * G;
-                                if (V == 1 || c4 < C4)
-                                    atomicAdd(out + c4, make_float4(acc[v][0], acc[v][1], acc[v][2], acc[v][3]));
+                                const float4 a4 = make_float4(acc[v][0], acc[v][1], acc[v][2], acc[v][3]);
+                                if (V == 1 || c4 < C4) {
+                                    if (own) out[c4] = a4;
+                                    else atomicAdd(out + c4, a4);
+                                }
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) acc[v][q] = 0.f;
                             }
+                            first_run = false;
                         }
                         cur = row[u];
                     }
@@ -442,6 +451,9 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
 {
     // columns [c0, c0 + cols) of every factor (a rank tile when cols < Rp)
     const int C4 = cols / 4;
+    // every row's nonzeros are contiguous in the slab when the mode is
+    // fiber-sorted (each row lies in one shard, sorted by row)
+    const int contiguous = (p.fiber && p.kclass[n] == 2) ? 1 : 0;
     const SlabPtrs sp = slab_in(in, p.N);
     float* out = p.Yhat[n] + c0;
     FacPtrs F = F0;
@@ -455,7 +467,8 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
     const dim3 grid(ntiles, split);
 #define DGPU_RUNT(G, V, TN)                                                                      \
     k_mttkrp_rowrun<N, G, V, BF, TN><<<grid, kRunThreads, 0, p.stream>>>(sp, tiles, F, out, n, \
-                                                                         w0, wl, cols, p.Rp)
+                                                                         w0, wl, cols, p.Rp,     \
+                                                                         contiguous)
 #define DGPU_RUN(G, V) DGPU_RUNT(G, V, -1)
     // target-mode specialisations for the common 3- and 4-mode, Rp <= 128 shapes
 #define DGPU_RUN_TGT(G)                                                       \
