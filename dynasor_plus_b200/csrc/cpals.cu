@@ -45,6 +45,10 @@ int launch_mttkrp_all_modes(Plan& p, const Slab& in);
 namespace {
 
 constexpr int kLaThreads = 256;
+#ifndef DGPU_SMALL_THREADS
+#define DGPU_SMALL_THREADS 1024
+#endif
+constexpr int kSmallThreads = DGPU_SMALL_THREADS;   // threads of the one-CTA factor update
 constexpr int kGramTile = 32;
 constexpr int kGramChunks = 296;           // 2 per SM
 
@@ -295,6 +299,31 @@ k_fit(const double* __restrict__ Gd, int N, int R, const double* __restrict__ la
     }
 }
 
+// The solve map of mode n alone (one warp): V = Hadamard of the other
+// modes' Grams, ridge, Cholesky, W -> Wout (FP64, entry (r, c) at
+// Wout[r * R + c]).  It depends only on the other modes' Grams, so it runs
+// on a side stream while mode n's MTTKRP runs.
+template <typename Real>
+__global__ void __launch_bounds__(32)
+k_small_solve(const double* __restrict__ Gd, int N, int n, int R, double ridge,
+              double* __restrict__ Wout)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int RR = R * R, LDA = R + 1;
+    double* Wx = reinterpret_cast<double*>(smraw);
+    Real* A = reinterpret_cast<Real*>(Wx + RR);
+    Real* invd = A + R * LDA;
+    for (int e = threadIdx.x; e < RR; e += 32) {
+        double v = 1.0;
+        for (int m = 0; m < N; ++m)
+            if (m != n) v *= Gd[(size_t)m * RR + e];
+        A[(e / R) * LDA + e % R] = (Real)v;
+    }
+    __syncwarp();
+    warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
+    for (int e = threadIdx.x; e < RR; e += 32) Wout[e] = Wx[e];
+}
+
 // The whole factor update of a small mode in one CTA (rows * Rp <= 8192,
 // R <= 64; the new factor is built in shared memory): Hadamard of the other Grams + relative ridge, Cholesky, the
 // solve map W, Y = Yhat W, the Gram of Y, lambda from its diagonal, the
@@ -308,7 +337,7 @@ __global__ void __launch_bounds__(1024)
 k_update_small(double* __restrict__ Gd, float* __restrict__ G32, int N, int n, int R, int Rp,
                double ridge, const float* __restrict__ Yhat, float* __restrict__ Y, uint32_t rows,
                float* __restrict__ lambda, double* __restrict__ lam64, int last, double tnorm2,
-               double* __restrict__ fitout)
+               double* __restrict__ fitout, const double* __restrict__ Wpre)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int RR = R * R;
@@ -327,17 +356,22 @@ k_update_small(double* __restrict__ Gd, float* __restrict__ G32, int N, int n, i
     for (uint32_t e = tid; e < total; e += nt) Hs[e] = __ldg(Yhat + e);
 
     for (int e = tid; e < RR; e += nt) {
-        double v = 1.0;
-        for (int m = 0; m < N; ++m)
-            if (m != n) v *= Gd[(size_t)m * RR + e];
-        A[(e / R) * LDA + e % R] = (Real)v;
+        if (Wpre) {
+            Wx[e] = Wpre[e];
+        } else {
+            double v = 1.0;
+            for (int m = 0; m < N; ++m)
+                if (m != n) v *= Gd[(size_t)m * RR + e];
+            A[(e / R) * LDA + e % R] = (Real)v;
+        }
         G[e] = 0.0;
     }
     for (int r = tid; r < R; r += nt) dot[r] = 0.0;
     __syncthreads();
     // ridge, Cholesky and the solve map in warp 0 alone (warp barriers
-    // only); the other warps wait at the next block barrier
-    if (tid < 32) warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
+    // only); the other warps wait at the next block barrier.  With Wpre the
+    // map was built by k_small_solve while this mode's MTTKRP ran.
+    if (!Wpre && tid < 32) warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
     __syncthreads();
     // Y = Yhat W (padding columns zero)
     for (uint32_t e = tid; e < total; e += nt) {
@@ -539,26 +573,51 @@ size_t small_update_smem(int R, int Rp, uint32_t rows, bool fp64) {
 
 // One ALS factor update of mode n from Yhat[n] (cpals.cpp:290-321).  For the
 // last mode *fit_done reports whether the fit was computed with it.
+bool small_mode(const Plan& p, int n) {
+    const uint64_t RR = (uint64_t)p.R * p.R;
+    return p.R <= 64 && (uint64_t)p.dims[n] * p.Rp <= 8192 && (uint64_t)p.dims[n] * RR <= (1ull << 21);
+}
+
+// The solve map of small mode n into L.Wd on stream `st` (k_small_solve).
+int launch_small_solve(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
+                       cudaStream_t st) {
+    const size_t RR = (size_t)p.R * p.R;
+    const size_t sm = RR * sizeof(double) + (size_t)p.R * (p.R + 2) * (solve_fp64 ? 8 : 4);
+    if (solve_fp64) {
+        if (sm > 48 * 1024)
+            DGPU_CUDA(cudaFuncSetAttribute(k_small_solve<double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_small_solve<double><<<1, 32, sm, st>>>(L.Gd, p.N, n, p.R, ridge, L.Wd);
+    } else {
+        if (sm > 48 * 1024)
+            DGPU_CUDA(cudaFuncSetAttribute(k_small_solve<float>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_small_solve<float><<<1, 32, sm, st>>>(L.Gd, p.N, n, p.R, ridge, L.Wd);
+    }
+    DGPU_CUDA(cudaGetLastError());
+    return DGPU_OK;
+}
+
 int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge, bool last,
-                double tn2, bool* fit_done) {
+                double tn2, bool* fit_done, const double* Wpre = nullptr) {
     const size_t RR = (size_t)p.R * p.R;
     *fit_done = false;
-    if (p.R <= 64 && (uint64_t)p.dims[n] * p.Rp <= 8192 && (uint64_t)p.dims[n] * RR <= (1ull << 21)) {
+    if (small_mode(p, n)) {
         const size_t sm = small_update_smem(p.R, p.Rp, p.dims[n], solve_fp64 != 0);
         if (solve_fp64) {
             if (sm > 48 * 1024)
                 DGPU_CUDA(cudaFuncSetAttribute(k_update_small<double>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_update_small<double><<<1, 1024, sm, p.stream>>>(
+            k_update_small<double><<<1, kSmallThreads, sm, p.stream>>>(
                 L.Gd, L.G32, p.N, n, p.R, p.Rp, ridge, p.Yhat[n], p.Y[n], p.dims[n], p.lambda,
-                L.lam64, last ? 1 : 0, tn2, L.fitout);
+                L.lam64, last ? 1 : 0, tn2, L.fitout, Wpre);
         } else {
             if (sm > 48 * 1024)
                 DGPU_CUDA(cudaFuncSetAttribute(k_update_small<float>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_update_small<float><<<1, 1024, sm, p.stream>>>(
+            k_update_small<float><<<1, kSmallThreads, sm, p.stream>>>(
                 L.Gd, L.G32, p.N, n, p.R, p.Rp, ridge, p.Yhat[n], p.Y[n], p.dims[n], p.lambda,
-                L.lam64, last ? 1 : 0, tn2, L.fitout);
+                L.lam64, last ? 1 : 0, tn2, L.fitout, Wpre);
         }
         DGPU_CUDA(cudaGetLastError());
         p.yb_stale[n] = true;
@@ -658,6 +717,7 @@ struct CpSession {
     double tn2 = 0.0;
     bool jacobi = false;
     std::vector<cudaEvent_t> ev;
+    std::vector<cudaEvent_t> fork, join;     // side-stream solve of each mode
     double* fit_host = nullptr;              // pinned: the per-iteration graphs' D2H target
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int cur_after[2] = {0, 0};
@@ -678,6 +738,8 @@ struct CpSession {
         : p(pl), o(op), res(r), fit_history(fh) {}
     ~CpSession() {
         for (auto e : ev) if (e) cudaEventDestroy(e);
+        for (auto e : fork) if (e) cudaEventDestroy(e);
+        for (auto e : join) if (e) cudaEventDestroy(e);
         if (fit_host) cudaFreeHost(fit_host);
         for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
         if (st) { dev_free(st); p.device_bytes -= st_bytes; }
@@ -700,6 +762,12 @@ struct CpSession {
         // ev[1] ends all MTTKRPs), ev[2 + 2n] end of mode n's factor update
         ev.assign(2 * p.N + 2, nullptr);
         for (auto& e : ev) DGPU_CUDA(cudaEventCreate(&e));
+        fork.assign(p.N, nullptr);
+        join.assign(p.N, nullptr);
+        for (auto& e : fork) DGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : join) DGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        if (!p.side_stream)
+            DGPU_CUDA(cudaStreamCreateWithFlags(&p.side_stream, cudaStreamNonBlocking));
         DGPU_CUDA(cudaMallocHost((void**)&fit_host, 4 * sizeof(double)));
         graphs = o.graphs != 0 && !p.timing;
         cur_start = p.cur;
@@ -742,10 +810,23 @@ struct CpSession {
             for (int n = 0; n < p.N; ++n)
                 DGPU_TRY(p.layout == DGPU_LAYOUT_NCOPY ? mode_ncopy(p, n) : mode_pingpong(p, n));
         for (int n = 0; n < p.N; ++n) {
+            // Gauss-Seidel on a small mode: its solve map depends only on the
+            // other modes' Grams, so it is built on the side stream while
+            // this mode's MTTKRP runs (fork after the previous update, join
+            // before this one)
+            const bool ovl = !jacobi && small_mode(p, n);
+            if (ovl) {
+                DGPU_CUDA(cudaEventRecord(fork[n], p.stream));
+                DGPU_CUDA(cudaStreamWaitEvent(p.side_stream, fork[n], 0));
+                DGPU_TRY(launch_small_solve(p, L, n, o.solve_fp64, o.ridge, p.side_stream));
+                DGPU_CUDA(cudaEventRecord(join[n], p.side_stream));
+            }
             if (!jacobi)
                 DGPU_TRY(p.layout == DGPU_LAYOUT_NCOPY ? mode_ncopy(p, n) : mode_pingpong(p, n));
             DGPU_CUDA(rec(1 + 2 * n));
-            DGPU_TRY(update_mode(p, L, n, o.solve_fp64, o.ridge, n == p.N - 1, tn2, &fit_done));
+            if (ovl) DGPU_CUDA(cudaStreamWaitEvent(p.stream, join[n], 0));
+            DGPU_TRY(update_mode(p, L, n, o.solve_fp64, o.ridge, n == p.N - 1, tn2, &fit_done,
+                                 ovl ? L.Wd : nullptr));
             DGPU_CUDA(rec(2 + 2 * n));
         }
         if (!fit_done) {

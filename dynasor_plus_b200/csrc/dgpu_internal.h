@@ -174,6 +174,7 @@ struct Plan {
     cudaStream_t stream = nullptr;
     bool         own_stream = false;
     cudaStream_t copy_stream = nullptr;         // host transfers overlapping the sweep
+    cudaStream_t side_stream = nullptr;         // CP-ALS solves overlapping the MTTKRP
     Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for

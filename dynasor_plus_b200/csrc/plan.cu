@@ -182,6 +182,7 @@ Plan::~Plan() {
     dev_free(la_work);
     dev_free(la_f32);
     if (copy_stream) { cudaStreamSynchronize(copy_stream); cudaStreamDestroy(copy_stream); }
+    if (side_stream) { cudaStreamSynchronize(side_stream); cudaStreamDestroy(side_stream); }
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
