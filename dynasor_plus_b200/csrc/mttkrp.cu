@@ -174,9 +174,11 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
         for (int k = 0; k < LPE; ++k) {
             const uint32_t e = gb + ch * CH + gl + k * G;
             const uint32_t p = tl.begin + (e < ge ? e : gb);
-            pf[k][0] = __float_as_uint(__ldg(in.vals + p));
+            // the slab is read once per sweep: streaming loads (evict first)
+            // keep L2 for the factor rows the gathers reuse
+            pf[k][0] = __float_as_uint(__ldcs(in.vals + p));
 #pragma unroll
-            for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldg(in.idx[w] + p);
+            for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldcs(in.idx[w] + p);
 #pragma unroll
             for (int f = 1 + N; f < SW; ++f) pf[k][f] = 0u;
         }
