@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--threads", type=int, default=16,
                     help="plan worker count: the FLYCOO geometry of the reference run with "
                          "this many threads (16 = the GPU host's cores)")
-    ap.add_argument("--layout", default="pingpong", choices=["pingpong", "ncopy"])
+    ap.add_argument("--layout", default="pingpong", choices=["pingpong", "ncopy", "auto"])
     ap.add_argument("--fiber", type=int, default=1)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"])
     ap.add_argument("--draws", type=int, default=DRAWS)
@@ -303,6 +303,7 @@ def main():
     plan = d.Plan(dims, vals, idx, threads=args.threads, rank=args.rank, layout=args.layout,
                   fiber=bool(args.fiber), precision=args.precision, device=local)
     build_s = time.time() - t0
+    layout_used = plan.info()["layout"]
     stream = torch.cuda.Stream(device=local)
     plan.set_stream(stream)
     Y = uniform_factors(dims, args.rank)
@@ -403,7 +404,7 @@ def main():
         "data": "synthetic",
         "config": {"workload": f"zipf{ZIPF_S} 3-mode {DIMS[0]}x{DIMS[1]}x{DIMS[2]}, {args.draws} draws "
                                f"deduped to {nnz} nnz, rank {args.rank}",
-                   "nnz": nnz, "layout": args.layout, "threads": args.threads,
+                   "nnz": nnz, "layout": layout_used, "threads": args.threads,
                    "fiber": bool(args.fiber), "precision": args.precision,
                    "l2": "inputs larger than L2 (slab %.2f GB)" % (nnz * (4 + 4 * N) / 1e9),
                    "parallelism": f"replicas x{ws}", "plan_build_s": round(build_s, 3)},
@@ -462,7 +463,7 @@ def main():
 
     # the same metric on the NCopy layout (one pre-sorted copy per mode, no
     # remap): the reference planner's choice when memory allows
-    if rank == 0 and args.layout == "pingpong" and not args.no_ncopy:
+    if rank == 0 and layout_used == "pingpong" and not args.no_ncopy:
         nc = d.Plan(dims, vals, idx, threads=args.threads, rank=args.rank, layout="ncopy",
                     fiber=bool(args.fiber), precision=args.precision, device=local)
         nc.set_stream(stream)

@@ -27,11 +27,13 @@ from ._lib import (CpOptions, CpResult, Coo, DgpuError, PlanInfo, PlanOpts, Tens
                    lib, LIB_PATH)
 
 __all__ = ["Plan", "DgpuError", "cpals_batch", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
-           "spmttkrp_dynasor", "device_count", "LIB_PATH", "PINGPONG", "NCOPY"]
+           "spmttkrp_dynasor", "device_count", "LIB_PATH", "PINGPONG", "NCOPY", "AUTO"]
 
 PINGPONG = 0
 NCOPY = 1
-LAYOUTS = {"pingpong": PINGPONG, "ncopy": NCOPY}
+AUTO = 2  # NCopy when its slabs fit the device-memory budget, else PingPong
+LAYOUTS = {"pingpong": PINGPONG, "ncopy": NCOPY, "auto": AUTO}
+LAYOUT_NAMES = {PINGPONG: "pingpong", NCOPY: "ncopy"}
 PRECISIONS = {"fp32": 0, "bf16": 1}
 ACCUMS = {"auto": 0, "rowrun": 1, "private": 2}
 
@@ -60,7 +62,9 @@ class Plan:
     idx    : N uint32 arrays of 0-based indices
     threads: the reference worker count the plan is built for (--threads)
     rank   : R; factors are I_n x padded_rank(R) float32
-    layout : "pingpong" (device remap every mode) or "ncopy"
+    layout : "pingpong" (device remap every mode), "ncopy", or "auto" (NCopy
+             when N+1 slabs fit 70% of free device memory less a headroom of
+             max(2 GiB, 25% of total), else PingPong; info()["layout"] tells)
     fiber  : fiber-sort DenseFiber modes (reference default) or not
              (the reference's DYN_FIBER_OFF=1 layout)
     precision: "fp32" or "bf16" (BF16 factor gathers, FP32 accumulation)
@@ -134,6 +138,7 @@ class Plan:
             "kernel_class": list(inf.kernel_class[:N]),
             "avg_fiber_len": list(inf.avg_fiber_len[:N]), "tiles": list(inf.tiles[:N]),
             "next_mode": inf.next_mode, "device_bytes": inf.device_bytes,
+            "layout": LAYOUT_NAMES.get(inf.layout, inf.layout),
         }
 
     def shards(self, n: int):

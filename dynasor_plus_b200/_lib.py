@@ -44,7 +44,7 @@ class PlanInfo(C.Structure):
                 ("mn_shift", C.c_int * MAX_MODES), ("shards_per_mode", C.c_uint32 * MAX_MODES),
                 ("kernel_class", C.c_int * MAX_MODES), ("avg_fiber_len", C.c_double * MAX_MODES),
                 ("tiles", C.c_uint32 * MAX_MODES), ("next_mode", C.c_int),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("layout", C.c_int)]
 
 
 class CpOptions(C.Structure):

@@ -103,7 +103,8 @@ int dgpu_plan_create(const dgpu_tensor_desc* t, const dgpu_plan_opts* o, dgpu_pl
     if (o->rank < 1 || o->rank > 1024) {
         set_error("dgpu_plan_create: rank %d outside [1,1024]", o->rank); return DGPU_ERR_ARG;
     }
-    if (o->layout != DGPU_LAYOUT_PINGPONG && o->layout != DGPU_LAYOUT_NCOPY) {
+    if (o->layout != DGPU_LAYOUT_PINGPONG && o->layout != DGPU_LAYOUT_NCOPY &&
+        o->layout != DGPU_LAYOUT_AUTO) {
         set_error("dgpu_plan_create: unknown layout %d", o->layout); return DGPU_ERR_ARG;
     }
     if (o->precision != DGPU_PREC_FP32 && o->precision != DGPU_PREC_BF16) {
@@ -159,6 +160,7 @@ int dgpu_plan_get_info(const dgpu_plan* plan, dgpu_plan_info* info) {
     }
     info->next_mode = p->next_mode;
     info->device_bytes = p->device_bytes;
+    info->layout = p->layout;
     return DGPU_OK;
 }
 

@@ -211,6 +211,30 @@ static uint32_t rows_per_shard(uint32_t I, int T) {
 }
 
 // ----------------------------------------------------------------------------
+//  layout from the device-memory budget (dyn_plan_storage,
+//  src/dynasor_preprocess.cpp:951-1104): the same rule with device memory in
+//  place of host RAM -- usable = 70% of free memory less a headroom of
+//  max(2 GiB, 25% of total); NCopy when its footprint plus overhead fits,
+//  else PingPong.
+// ----------------------------------------------------------------------------
+static int choose_layout(Plan& p) {
+    size_t free_b = 0, total_b = 0;
+    DGPU_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double slab = (double)p.nnz * (4.0 + 4.0 * p.N) + 256.0 * (p.N + 1);
+    double factors = 0.0;
+    for (int n = 0; n < p.N; ++n)
+        factors += (double)p.dims[n] * p.Rp * 4.0 * (p.precision == DGPU_PREC_BF16 ? 2.5 : 2.0);
+    // partition scratch (chunk x bucket tables) and slack
+    const double overhead = factors + 64.0 * 1024 * 1024 + 0.05 * slab;
+    const double headroom = std::max(2.0 * (1ull << 30), 0.25 * (double)total_b);
+    const double usable = 0.70 * (double)free_b;
+    const double budget = usable > headroom ? usable - headroom : 0.0;
+    const double ncopy_need = (double)(p.N + 1) * slab + overhead;
+    p.layout = ncopy_need <= budget ? DGPU_LAYOUT_NCOPY : DGPU_LAYOUT_PINGPONG;
+    return DGPU_OK;
+}
+
+// ----------------------------------------------------------------------------
 //  device: per-mode shard histograms + index range check
 // ----------------------------------------------------------------------------
 struct Geom {
@@ -360,6 +384,8 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
         p.afl[n] = (double)p.nnz / (double)std::max<uint32_t>(1u, p.dims[n]);
         p.kclass[n] = p.afl[n] >= 32.0 ? 2 : (p.afl[n] >= 8.0 ? 1 : 0);
     }
+
+    if (p.layout == DGPU_LAYOUT_AUTO) DGPU_TRY(choose_layout(p));
 
     // slabs: PingPong keeps primary + scratch; NCopy keeps N copies (+1
     // scratch while sorting).

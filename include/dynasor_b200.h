@@ -49,6 +49,10 @@ extern "C" {
 /* ---- layouts / kernels (values match the reference enums) ------------ */
 #define DGPU_LAYOUT_PINGPONG 0   /* Layout::PingPong: remap every mode    */
 #define DGPU_LAYOUT_NCOPY    1   /* Layout::NCopy: N pre-sorted copies    */
+/* Layout chosen from the device-memory budget like dyn_plan_storage
+ * (src/dynasor_preprocess.cpp:951-1104): NCopy when it fits, else PingPong.
+ * dgpu_plan_info.layout reports the choice. */
+#define DGPU_LAYOUT_AUTO     2
 
 #define DGPU_CP_GAUSS_SEIDEL 0   /* CpKernel::GaussSeidel                 */
 #define DGPU_CP_JACOBI       1   /* CpKernel::Jacobi (all-modes pass)     */
@@ -108,6 +112,7 @@ typedef struct {
     uint32_t  tiles[DGPU_MAX_MODES];            /* device work tiles      */
     int       next_mode;                        /* mode the slab is ready for */
     uint64_t  device_bytes;                     /* HBM held by the plan   */
+    int       layout;                           /* DGPU_LAYOUT_PINGPONG / NCOPY in use */
 } dgpu_plan_info;
 
 /* CP-ALS options / result (mirror CpOptions / CpResult,

@@ -74,7 +74,8 @@ def test_gradient_vs_finite_differences(bindings):
     F = CpOptLoss.build(p, vals, R)
     Ys = [torch.tensor(y, requires_grad=True) for y in Y]
     loss = F.apply(*Ys)
-    assert abs(float(loss) - _loss64(bindings, idx, vals, Y, R)) < 1e-3 * max(1.0, abs(float(loss)))
+    lv = float(loss.detach())
+    assert abs(lv - _loss64(bindings, idx, vals, Y, R)) < 1e-3 * max(1.0, abs(lv))
     loss.backward()
     rng = np.random.default_rng(0)
     h = 1e-4

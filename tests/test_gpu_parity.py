@@ -243,3 +243,34 @@ def test_host_sweep_overlapped_transfers_match_device_sweep(layout):
         for n in range(3):
             assert rel_fro(out[n], ref[n]) < 1e-6
     p.close()
+
+
+def test_auto_layout_picks_ncopy_when_it_fits():
+    """layout="auto" resolves to NCopy for a tensor whose N+1 slabs fit the
+    device-memory budget, and then holds the same copies and Yhat as an
+    explicit NCopy plan (copies bit-exact; Yhat up to the order of the FP32
+    atomics at row-run boundaries)."""
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.zipf((3000, 500, 200), draws=30000, s=1.1, seed=31)
+    T, R = 4, 16
+    a = _plan(dims, vals, idx, T, R, layout="auto")
+    b = _plan(dims, vals, idx, T, R, layout="ncopy")
+    assert a.info()["layout"] == "ncopy"
+    assert b.info()["layout"] == "ncopy"
+    assert _plan(dims, vals, idx, T, R, layout="pingpong").info()["layout"] == "pingpong"
+    rng = np.random.default_rng(5)
+    for n in range(3):
+        y = rng.uniform(-1, 1, (int(dims[n]), a.Rp)).astype(np.float32)
+        a.set_factor(n, y)
+        b.set_factor(n, y)
+    for n in range(3):
+        av, aix = a.copy(n)
+        bv, bix = b.copy(n)
+        assert np.array_equal(av, bv) and all(np.array_equal(x, y) for x, y in zip(aix, bix))
+    a.sweep()
+    b.sweep()
+    for n in range(3):
+        assert rel_fro(a.yhat(n), b.yhat(n)) < 1e-6, n
+    a.close()
+    b.close()
