@@ -57,6 +57,9 @@ constexpr int kHistThreads = 1024;
 #endif
 constexpr int kScatThreads = DGPU_SCAT_THREADS;   // threads of a scatter CTA
 constexpr int kScatWarps = kScatThreads / 32;
+// Thread that issues a scatter CTA's bulk copies: the last one, whose warp
+// has no bucket-prefix work for up to kScatThreads / 2 buckets.
+constexpr int kIssuer = kScatThreads - 1;
 constexpr uint32_t kSegChunkTiles = 16;       // <= 64K elements per segmented chunk
 
 __device__ __forceinline__ uint32_t part_key(uint32_t v, int shift, uint32_t mask) {
@@ -226,16 +229,23 @@ __device__ __forceinline__ void fence_mbar_init() {
 constexpr int kErrPartWait = 0x100;      // a bulk copy did not complete in time
 constexpr int kErrPartRange = 0x200;     // a slot outside its window or slab (skipped)
 
+// Tile descriptors of a chunk that a scatter CTA copies to shared memory
+// when it takes the chunk (a chunk with more tiles reads the rest from
+// global memory).
+constexpr uint32_t kTileStage = 64;
+
 // Next non-empty window of a chunk after (t, w0): windows are W-element
 // pieces of the chunk's tiles in order.  Returns false at the chunk's end.
+// Tiles tb .. tb + kTileStage - 1 come from the shared copy `st`.
 template <int W>
-__device__ __forceinline__ bool next_window(const Tile* __restrict__ tiles, uint32_t tend,
-                                            uint32_t& t, uint32_t& w0, Tile& tl)
+__device__ __forceinline__ bool next_window(const Tile* __restrict__ tiles, const Tile* st,
+                                            uint32_t tb, uint32_t tend, uint32_t& t, uint32_t& w0,
+                                            Tile& tl)
 {
     w0 += W;
     while (w0 >= tl.count) {
         if (++t >= tend) return false;
-        tl = tiles[t];
+        tl = (t - tb < kTileStage) ? st[t - tb] : tiles[t];
         w0 = 0;
     }
     return true;
@@ -259,6 +269,31 @@ __device__ __forceinline__ void issue_window(uint32_t* buf, const SlabPtrs& in, 
     bulk_g2s(buf, in.vals + a, bytes, bar);
 #pragma unroll
     for (int k = 0; k < N; ++k) bulk_g2s(buf + (size_t)(k + 1) * BW, in.idx[k] + a, bytes, bar);
+}
+
+// Per-warp 16-bit bucket counters, bucket-major: bucket b's 16 counters
+// (one per warp) fill the 32 bytes at b * 16, so one thread reads and
+// rewrites a bucket's counters with two 16-byte accesses.  The pair of warps
+// (2j, 2j+1) sits in word j ^ (b & 7) of the row, which spreads the lanes of
+// one warp that touch different buckets over all 32 banks.
+__device__ __forceinline__ uint32_t wc_slot(uint32_t b, int warp) {
+    return b * 16u + (((((uint32_t)warp >> 1) ^ (b & 7u))) << 1) + ((uint32_t)warp & 1u);
+}
+
+// Row of bucket b <-> the 8 words in warp-pair order: word j and j ^ (b & 7)
+// swap places (an involution, so the same call maps both ways).
+__device__ __forceinline__ void wc_unswizzle(uint32_t (&u)[8], uint32_t b) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const bool sw = (b >> k) & 1u;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (j & (1 << k)) continue;
+            const uint32_t a = u[j], c = u[j | (1 << k)];
+            u[j] = sw ? c : a;
+            u[j | (1 << k)] = sw ? a : c;
+        }
+    }
 }
 
 // Window size of the scatter and its buffer column count: N+1 input
@@ -302,16 +337,17 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t wsum[kScatWarps];
     __shared__ uint32_t s_chunk[2];     // alternating: a slot is rewritten two barriers later
+    __shared__ Tile s_tiles[kTileStage];
     __shared__ int fail;
     const uint32_t nbp = (nb + 7u) & ~7u;
     uint32_t* buf = sm;                                      // [2][C][BW]
     uint32_t* cursor = buf + 2 * C * BW;                     // [nbp]
     uint2* ld = reinterpret_cast<uint2*>(cursor + nbp);      // [nbp] {window base, dest - slot}
-    uint16_t* wc = reinterpret_cast<uint16_t*>(ld + nbp);    // [16][nbp]
+    uint16_t* wc = reinterpret_cast<uint16_t*>(ld + nbp);    // [nbp][16], see wc_slot
+    static_assert(kScatWarps == 16, "bucket counter rows hold 16 warps");
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    uint16_t* mywc = wc + (size_t)warp * nbp;
     for (uint32_t i = threadIdx.x; i < kScatWarps * nbp / 2; i += blockDim.x)
         reinterpret_cast<uint32_t*>(wc)[i] = 0;
     if (threadIdx.x == 0) {
@@ -333,12 +369,15 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
         const uint32_t* o = off + (size_t)ci * nb;
         const uint32_t* bs = base + (size_t)c.seg * nb;
         for (uint32_t b = threadIdx.x; b < nb; b += blockDim.x) cursor[b] = o[b] + bs[b];
-        // first non-empty window of the chunk
         if (c.tile_begin >= c.tile_end) continue;
+        const uint32_t nst = min(kTileStage, c.tile_end - c.tile_begin);
+        for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_tiles[i] = tiles[c.tile_begin + i];
+        __syncthreads();           // tile descriptors staged
+        // first non-empty window of the chunk
         uint32_t t = c.tile_begin, w0 = 0u - (uint32_t)W;
-        Tile tl = tiles[t];
-        if (!next_window<W>(tiles, c.tile_end, t, w0, tl)) continue;
-        if (threadIdx.x == 0)
+        Tile tl = s_tiles[0];
+        if (!next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, t, w0, tl)) continue;
+        if (threadIdx.x == kIssuer)
             issue_window<N, W>(buf + (size_t)(kw & 1) * C * BW, in, tl.begin + w0,
                                min((uint32_t)W, tl.count - w0), &bar[kw & 1]);
         pending = true;
@@ -373,9 +412,10 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                 rk[s] = 0;
                 if (act) {
                     const unsigned peers = __match_any_sync(am, key[s]);
-                    const uint32_t prior = mywc[key[s]];
+                    const uint32_t slot = wc_slot(key[s], warp);
+                    const uint32_t prior = wc[slot];
                     __syncwarp(am);
-                    if ((peers & lt) == 0) mywc[key[s]] = (uint16_t)(prior + __popc(peers));
+                    if ((peers & lt) == 0) wc[slot] = (uint16_t)(prior + __popc(peers));
                     rk[s] = prior + __popc(peers & lt);
                 }
                 __syncwarp();
@@ -387,8 +427,8 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             // (window kw-1's write-out) finished before barrier (1)
             uint32_t nt = t, nw0 = w0;
             Tile ntl = tl;
-            const bool more = next_window<W>(tiles, c.tile_end, nt, nw0, ntl);
-            if (more && threadIdx.x == 0)
+            const bool more = next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, nt, nw0, ntl);
+            if (more && threadIdx.x == kIssuer)
                 issue_window<N, W>(buf + (size_t)((kw + 1) & 1) * C * BW, in, ntl.begin + nw0,
                                    min((uint32_t)W, ntl.count - nw0), &bar[(kw + 1) & 1]);
             // b. warp prefixes per bucket (only counters a warp used become
@@ -402,13 +442,23 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                 tot[u] = 0;
                 const uint32_t b = b0 + u;
                 if ((uint32_t)u < per && b < nb) {
+                    uint4* row = reinterpret_cast<uint4*>(wc + (size_t)b * 16);
+                    const uint4 q0 = row[0], q1 = row[1];
+                    uint32_t r8[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+                    wc_unswizzle(r8, b);
                     uint32_t run = 0;
 #pragma unroll
-                    for (int w = 0; w < kScatWarps; ++w) {
-                        const uint32_t v = wc[(size_t)w * nbp + b];
-                        if (v) wc[(size_t)w * nbp + b] = (uint16_t)run;
-                        run += v;
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t lo = r8[j] & 0xffffu, hi = r8[j] >> 16;
+                        const uint32_t plo = lo ? run : 0u;
+                        run += lo;
+                        const uint32_t phi = hi ? run : 0u;
+                        run += hi;
+                        r8[j] = plo | (phi << 16);
                     }
+                    wc_unswizzle(r8, b);
+                    row[0] = make_uint4(r8[0], r8[1], r8[2], r8[3]);
+                    row[1] = make_uint4(r8[4], r8[5], r8[6], r8[7]);
                     tot[u] = run;
                     sum += run;
                 }
@@ -443,7 +493,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
                 const uint2 bd = ld[key[s]];
-                const uint32_t lp = bd.x + mywc[key[s]] + rk[s];
+                const uint32_t lp = bd.x + wc[wc_slot(key[s], warp)] + rk[s];
                 if (lp >= cnt) { atomicOr(err, kErrPartRange); continue; }
                 if constexpr (kRec) {
                     uint32_t r[4] = {__float_as_uint(val[s]), 0u, 0u, 0u};
@@ -460,7 +510,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             __syncwarp();
 #pragma unroll
             for (int s = 0; s < S; ++s)
-                if (key[s] != 0xffffffffu) mywc[key[s]] = 0;
+                if (key[s] != 0xffffffffu) wc[wc_slot(key[s], warp)] = 0;
             __syncthreads();       // (4)
             // d. write-out: runs of one bucket are contiguous
             for (uint32_t i = threadIdx.x; i < cnt; i += kScatThreads) {
@@ -487,7 +537,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
         if (fail) break;
     }
     // leave no bulk copy in flight into this CTA's shared memory
-    if (fail && pending && threadIdx.x == 0) mbar_wait(&bar[kw & 1], (kw >> 1) & 1u);
+    if (fail && pending && threadIdx.x == kIssuer) mbar_wait(&bar[kw & 1], (kw >> 1) & 1u);
 }
 
 
