@@ -23,10 +23,11 @@ import os
 
 import numpy as np
 
-from ._lib import (CpOptions, CpResult, Coo, DgpuError, PlanInfo, PlanOpts, TensorDesc, check,
+from ._lib import (CpOptions, CpResult, Coo, DgpuError, DnpInfo, PlanInfo, PlanOpts, TensorDesc, check,
                    lib, LIB_PATH)
 
 __all__ = ["Plan", "DgpuError", "cpals_batch", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
+           "dnp_peek",
            "spmttkrp_dynasor", "device_count", "LIB_PATH", "PINGPONG", "NCOPY", "AUTO"]
 
 PINGPONG = 0
@@ -107,6 +108,43 @@ class Plan:
         self._idx = None
         if stream is not None:
             self.set_stream(stream)
+
+    @classmethod
+    def from_dnp(cls, path, threads: int, rank: int, precision: str = "fp32", device: int = 0,
+                 stream=None, accum: str = "auto", fiber: bool = True) -> "Plan":
+        """A plan from a .dnp processed-tensor file (the reference's
+        runtime-only mode, load_dnp_tensor): its slab(s), shard tables and
+        schedule are used as they are.  `threads` must equal the file's
+        thread count; the file decides the layout (PingPong or NCopy).
+        `fiber` applies to PingPong files (NCopy copies record it)."""
+        L = lib()
+        info = dnp_peek(path)
+        self = cls.__new__(cls)
+        self.N = info["num_modes"]
+        self.dims = np.asarray(info["mode_size"], np.uint32)
+        self.nnz = info["nnz"]
+        self.R = int(rank)
+        self.Rp = padded_rank(rank)
+        self._vals = self._idx = self._mn = None
+        opts = PlanOpts()
+        L.dgpu_plan_opts_default(C.byref(opts))
+        opts.threads = int(threads)
+        opts.rank = self.R
+        opts.fiber = 1 if fiber else 0
+        opts.precision = PRECISIONS[precision]
+        opts.device = int(device)
+        opts.accum = ACCUMS[accum]
+        h = C.c_void_p()
+        check(L.dgpu_plan_create_from_dnp(os.fsencode(path), C.byref(opts), C.byref(h)))
+        self._h = h
+        if stream is not None:
+            self.set_stream(stream)
+        return self
+
+    def save_dnp(self, path):
+        """Write the plan as a .dnp file (save_dnp_tensor): PingPong plans
+        between sweeps, NCopy plans any time."""
+        check(lib().dgpu_plan_save_dnp(self._h, os.fsencode(path)))
 
     # -- lifetime -----------------------------------------------------------
     def close(self):
@@ -351,6 +389,21 @@ def load_dnb(path: str):
         return _coo_to_numpy(c)
     finally:
         lib().dgpu_coo_free(C.byref(c))
+
+
+DNP_LAYOUTS = {0: "morton", 1: "ncopy", 2: "pingpong", 3: "inplace"}
+
+
+def dnp_peek(path) -> dict:
+    """Header of a .dnp processed-tensor file (no device needed):
+    layout, num_modes, nnz, mode_size and the thread count its schedule was
+    built for (load_dnp_header / load_dnp_num_threads / load_dnp_layout)."""
+    info = DnpInfo()
+    check(lib().dgpu_dnp_peek(os.fsencode(path), C.byref(info)))
+    N = info.num_modes
+    return {"layout": DNP_LAYOUTS.get(info.layout_kind, info.layout_kind), "num_modes": N,
+            "nnz": int(info.nnz), "mode_size": list(info.mode_size[:N]),
+            "num_threads": info.num_threads}
 
 
 def save_dnb_tensor(path: str, dims, vals, idx):

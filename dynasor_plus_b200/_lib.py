@@ -47,6 +47,11 @@ class PlanInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("layout", C.c_int)]
 
 
+class DnpInfo(C.Structure):
+    _fields_ = [("layout_kind", C.c_int), ("num_modes", C.c_int), ("nnz", C.c_uint64),
+                ("mode_size", C.c_uint32 * MAX_MODES), ("num_threads", C.c_int)]
+
+
 class CpOptions(C.Structure):
     _fields_ = [("max_iters", C.c_int), ("tol", C.c_double), ("seed", C.c_uint64),
                 ("ridge", C.c_double), ("kernel", C.c_int), ("solve_fp64", C.c_int),
@@ -77,6 +82,9 @@ _SIGS = {
     "dgpu_plan_opts_default": (None, [C.POINTER(PlanOpts)]),
     "dgpu_plan_create": (C.c_int, [C.POINTER(TensorDesc), C.POINTER(PlanOpts), C.POINTER(C.c_void_p)]),
     "dgpu_plan_destroy": (C.c_int, [C.c_void_p]),
+    "dgpu_dnp_peek": (C.c_int, [C.c_char_p, C.POINTER(DnpInfo)]),
+    "dgpu_plan_create_from_dnp": (C.c_int, [C.c_char_p, C.POINTER(PlanOpts), C.POINTER(C.c_void_p)]),
+    "dgpu_plan_save_dnp": (C.c_int, [C.c_void_p, C.c_char_p]),
     "dgpu_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "dgpu_plan_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dgpu_plan_sync": (C.c_int, [C.c_void_p]),

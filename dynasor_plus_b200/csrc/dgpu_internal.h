@@ -230,6 +230,38 @@ int timing_collect(Plan& p);
 // reported as DGPU_ERR_DEVICE.
 int sync_checked(Plan& p);
 
+// ---- .dnp processed-tensor image (src/dynasor_dnp.cpp) ---------------------
+// Host copy of everything one .dnp file holds for the PingPong and NCopy
+// layouts.  `copies` slabs: 1 for PingPong, N for NCopy.
+struct DnpImage {
+    int      layout = DGPU_LAYOUT_PINGPONG;      // DGPU_LAYOUT_PINGPONG / NCOPY
+    int      N = 0;
+    uint64_t nnz = 0;
+    uint32_t dims[kMaxModes] = {};
+    int      threads = 0;
+    double   tnorm_sq = 0.0;
+    uint32_t K[kMaxModes] = {};
+    uint32_t mn[kMaxModes] = {};
+    int32_t  shift[kMaxModes] = {};
+    uint32_t shard_size = 0;
+    double   afl[kMaxModes] = {};
+    uint32_t kclass[kMaxModes] = {};
+    int8_t   inplace_mode = 0;
+    uint64_t remap_stride = 0;
+    std::vector<uint64_t> touched_count;                      // [n]
+    std::vector<std::vector<uint8_t>> touched;                // [n][ceil(I_n/8)]
+    std::vector<std::vector<uint64_t>> sbeg, send;            // [n][s]
+    std::vector<std::vector<std::vector<uint32_t>>> sched;    // [n][tid]
+    std::vector<std::vector<uint64_t>> cursor;                // [n][tid * stride + s']
+    uint8_t  fiber_sorted[kMaxModes] = {};
+    uint8_t  csr[kMaxModes] = {};
+    std::vector<float> vals[kMaxModes];                       // [copy][nnz]
+    std::vector<uint32_t> idx[kMaxModes][kMaxModes];          // [copy][mode][nnz]
+    std::vector<uint64_t> rowptr[kMaxModes];                  // [copy][I_k + 1] when csr[k]
+};
+// A plan that uses the image's slabs, shard tables and schedule as they are.
+int plan_build_dnp(Plan& p, const DnpImage& img, const dgpu_plan_opts& o);
+
 // ---- device memory helpers ----------------------------------------------
 int  dev_alloc(Plan& p, void** ptr, size_t bytes);
 void dev_free(void* ptr);

@@ -348,9 +348,10 @@ static int build_fiber_tiles(Plan& p, int n) {
 // ----------------------------------------------------------------------------
 //  plan creation
 // ----------------------------------------------------------------------------
-int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
-    p.N = t.num_modes;
-    p.nnz = t.nnz;
+// Scalars, stream and tuning knobs shared by both ways of building a plan.
+static int plan_init(Plan& p, int N, uint64_t nnz, const uint32_t* dims, const dgpu_plan_opts& o) {
+    p.N = N;
+    p.nnz = nnz;
     p.T = o.threads;
     p.R = o.rank;
     p.Rp = (o.rank + 15) / 16 * 16;
@@ -370,25 +371,25 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     if (const char* e = std::getenv("DGPU_SORT_DIGIT_BITS")) p.sort_digit_bits = std::atoi(e);
     if (const char* e = std::getenv("DGPU_FIBER_DIGIT_BITS")) p.fiber_digit_bits = std::atoi(e);
     if (const char* e = std::getenv("DGPU_RANK_TILE")) p.rank_tile = std::atoi(e);
+    for (int n = 0; n < N; ++n) p.dims[n] = dims[n];
+    return DGPU_OK;
+}
 
-    // geometry
-    for (int n = 0; n < p.N; ++n) {
-        p.dims[n] = t.mode_size[n];
-        uint32_t mn;
-        if (o.mn_target && o.mn_target[n] > 0) mn = round_up_pow2(o.mn_target[n]);
-        else mn = rows_per_shard(p.dims[n], p.T);
-        p.mn[n] = mn;
-        p.shift[n] = log2_ceil(mn);
-        p.K[n] = (p.dims[n] + mn - 1) / mn;
-        if (p.K[n] == 0) p.K[n] = 1;
-        p.afl[n] = (double)p.nnz / (double)std::max<uint32_t>(1u, p.dims[n]);
-        p.kclass[n] = p.afl[n] >= 32.0 ? 2 : (p.afl[n] >= 8.0 ? 1 : 0);
-    }
+// Shard geometry of mode n for `mn` (a power of two) rows per shard, and the
+// kernel class from the average fiber length (src/dynasor_preprocess.cpp:
+// 2087-2095).
+static void plan_mode_geometry(Plan& p, int n, uint32_t mn) {
+    p.mn[n] = mn;
+    p.shift[n] = log2_ceil(mn);
+    p.K[n] = (p.dims[n] + mn - 1) / mn;
+    if (p.K[n] == 0) p.K[n] = 1;
+    p.afl[n] = (double)p.nnz / (double)std::max<uint32_t>(1u, p.dims[n]);
+    p.kclass[n] = p.afl[n] >= 32.0 ? 2 : (p.afl[n] >= 8.0 ? 1 : 0);
+}
 
-    if (p.layout == DGPU_LAYOUT_AUTO) DGPU_TRY(choose_layout(p));
-
-    // slabs: PingPong keeps primary + scratch; NCopy keeps N copies (+1
-    // scratch while sorting).
+// Slabs: PingPong keeps primary + scratch; NCopy keeps N copies (+1 scratch
+// while sorting).
+static int plan_alloc_slabs(Plan& p) {
     const int nslab = (p.layout == DGPU_LAYOUT_NCOPY) ? std::max(p.N + 1, 2) : 2;
     if (nslab > kMaxModes) {
         set_error("NCopy with %d modes needs %d slabs (max %d)", p.N, nslab, kMaxModes);
@@ -398,16 +399,12 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     DGPU_TRY(dev_alloc(p, (void**)&p.err_flag, sizeof(int)));
     DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
     DGPU_TRY(dev_alloc(p, (void**)&p.part_ctr, sizeof(uint32_t)));
+    return DGPU_OK;
+}
 
-    // input COO -> slab[1] (the reference's loader order)
-    const int in_slab = 1;
-    DGPU_CUDA(cudaMemcpyAsync(p.slab[in_slab].vals, t.vals, p.nnz * sizeof(float),
-                              cudaMemcpyHostToDevice, p.stream));
-    for (int n = 0; n < p.N; ++n)
-        DGPU_CUDA(cudaMemcpyAsync(p.slab[in_slab].idx[n], t.idx[n], p.nnz * sizeof(uint32_t),
-                                  cudaMemcpyHostToDevice, p.stream));
-
-    // shard histograms on the device
+// Per-mode shard histograms of slab `s` on the device (any element order),
+// with every index checked against its mode size.
+static int device_shard_counts(Plan& p, const Slab& s, std::vector<std::vector<uint64_t>>& out) {
     Geom g{};
     uint32_t total = 0;
     for (int n = 0; n < p.N; ++n) {
@@ -419,11 +416,12 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     unsigned long long* counts_d = nullptr;
     DGPU_TRY(dev_alloc(p, (void**)&counts_d, (size_t)total * 8));
     DGPU_CUDA(cudaMemsetAsync(counts_d, 0, (size_t)total * 8, p.stream));
+    DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
     const int use_smem = total <= 12288 ? 1 : 0;
     const unsigned blocks =
         (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((p.nnz + 255) / 256, 148 * 8));
     k_shard_counts<<<blocks, 256, use_smem ? total * 4 : 0, p.stream>>>(
-        slab_in(p.slab[in_slab], p.N), p.N, p.nnz, g, total, use_smem, counts_d, p.err_flag);
+        slab_in(s, p.N), p.N, p.nnz, g, total, use_smem, counts_d, p.err_flag);
     DGPU_CUDA(cudaGetLastError());
     std::vector<unsigned long long> counts_h(total);
     int err_h = 0;
@@ -433,16 +431,81 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     DGPU_CUDA(cudaStreamSynchronize(p.stream));
     dev_free(counts_d);
     p.device_bytes -= (size_t)total * 8;
+    DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
     if (err_h) {
         set_error("plan: an index is out of range of its mode size");
         return DGPU_ERR_INDEX;
     }
+    out.assign(p.N, {});
+    for (int n = 0; n < p.N; ++n)
+        out[n].assign(counts_h.begin() + g.binoff[n], counts_h.begin() + g.binoff[n] + p.K[n]);
+    return DGPU_OK;
+}
 
-    p.count.assign(p.N, {});
+// Tiles, partition lists and fiber tile lists from the shard tables and the
+// schedule.
+static int plan_tables(Plan& p) {
+    build_tiles(p);
+    static const std::vector<uint32_t> kNone;
+    for (int n = 0; n < p.N; ++n) {
+        DGPU_TRY(upload_tiles(p, p.tiles_h[n], &p.tiles_d[n]));
+        DGPU_TRY(build_partlist(p, p.tiles_h[n], kNone, kNone, p.proc[n], p.tiles_d[n]));
+    }
+    for (int n = 0; n < p.N; ++n)
+        if (p.fiber && p.kclass[n] == 2) DGPU_TRY(build_fiber_tiles(p, n));
+    std::vector<Tile> id;
+    for (uint64_t x = 0; x < p.nnz; x += kTile) {
+        Tile tl;
+        tl.begin = (uint32_t)x;
+        tl.count = (uint32_t)std::min<uint64_t>(kTile, p.nnz - x);
+        tl.shard = 0;
+        tl.seg_first = 0;
+        id.push_back(tl);
+    }
+    return build_partlist(p, id, kNone, kNone, p.ident, nullptr);
+}
+
+static int plan_factors(Plan& p) {
+    for (int n = 0; n < p.N; ++n) {
+        const size_t fb = (size_t)p.dims[n] * p.Rp * sizeof(float);
+        DGPU_TRY(dev_alloc(p, (void**)&p.Y[n], fb));
+        DGPU_TRY(dev_alloc(p, (void**)&p.Yhat[n], fb));
+        DGPU_CUDA(cudaMemsetAsync(p.Y[n], 0, fb, p.stream));
+        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, fb, p.stream));
+        if (p.precision == DGPU_PREC_BF16) {
+            DGPU_TRY(dev_alloc(p, (void**)&p.Yb[n], fb / 2));
+            DGPU_CUDA(cudaMemsetAsync(p.Yb[n], 0, fb / 2, p.stream));
+        }
+        p.yb_stale[n] = true;
+    }
+    DGPU_TRY(dev_alloc(p, (void**)&p.lambda, (size_t)p.Rp * sizeof(float)));
+    return DGPU_OK;
+}
+
+int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
+    DGPU_TRY(plan_init(p, t.num_modes, t.nnz, t.mode_size, o));
+    // geometry
+    for (int n = 0; n < p.N; ++n) {
+        const uint32_t mn = (o.mn_target && o.mn_target[n] > 0) ? round_up_pow2(o.mn_target[n])
+                                                                : rows_per_shard(p.dims[n], p.T);
+        plan_mode_geometry(p, n, mn);
+    }
+    if (p.layout == DGPU_LAYOUT_AUTO) DGPU_TRY(choose_layout(p));
+    DGPU_TRY(plan_alloc_slabs(p));
+
+    // input COO -> slab[1] (the reference's loader order)
+    const int in_slab = 1;
+    DGPU_CUDA(cudaMemcpyAsync(p.slab[in_slab].vals, t.vals, p.nnz * sizeof(float),
+                              cudaMemcpyHostToDevice, p.stream));
+    for (int n = 0; n < p.N; ++n)
+        DGPU_CUDA(cudaMemcpyAsync(p.slab[in_slab].idx[n], t.idx[n], p.nnz * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice, p.stream));
+
+    // shard histograms on the device -> shard tables, schedule, tiles
+    DGPU_TRY(device_shard_counts(p, p.slab[in_slab], p.count));
     p.sbeg.assign(p.N, {});
     p.send.assign(p.N, {});
     for (int n = 0; n < p.N; ++n) {
-        p.count[n].assign(counts_h.begin() + g.binoff[n], counts_h.begin() + g.binoff[n] + p.K[n]);
         p.sbeg[n].resize(p.K[n]);
         p.send[n].resize(p.K[n]);
         uint64_t c = 0;
@@ -453,26 +516,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
         }
     }
     build_schedule(p);
-    build_tiles(p);
-    static const std::vector<uint32_t> kNone;
-    for (int n = 0; n < p.N; ++n) {
-        DGPU_TRY(upload_tiles(p, p.tiles_h[n], &p.tiles_d[n]));
-        DGPU_TRY(build_partlist(p, p.tiles_h[n], kNone, kNone, p.proc[n], p.tiles_d[n]));
-    }
-    for (int n = 0; n < p.N; ++n)
-        if (p.fiber && p.kclass[n] == 2) DGPU_TRY(build_fiber_tiles(p, n));
-    {
-        std::vector<Tile> id;
-        for (uint64_t x = 0; x < p.nnz; x += kTile) {
-            Tile tl;
-            tl.begin = (uint32_t)x;
-            tl.count = (uint32_t)std::min<uint64_t>(kTile, p.nnz - x);
-            tl.shard = 0;
-            tl.seg_first = 0;
-            id.push_back(tl);
-        }
-        DGPU_TRY(build_partlist(p, id, kNone, kNone, p.ident, nullptr));
-    }
+    DGPU_TRY(plan_tables(p));
 
     // stable scatter of the input order into mode-0 shard order
     int res = 0;
@@ -508,21 +552,173 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
             }
         }
     }
+    DGPU_TRY(plan_factors(p));
+    DGPU_TRY(sync_checked(p));
+    return DGPU_OK;
+}
 
-    // factors
-    for (int n = 0; n < p.N; ++n) {
-        const size_t fb = (size_t)p.dims[n] * p.Rp * sizeof(float);
-        DGPU_TRY(dev_alloc(p, (void**)&p.Y[n], fb));
-        DGPU_TRY(dev_alloc(p, (void**)&p.Yhat[n], fb));
-        DGPU_CUDA(cudaMemsetAsync(p.Y[n], 0, fb, p.stream));
-        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, fb, p.stream));
-        if (p.precision == DGPU_PREC_BF16) {
-            DGPU_TRY(dev_alloc(p, (void**)&p.Yb[n], fb / 2));
-            DGPU_CUDA(cudaMemsetAsync(p.Yb[n], 0, fb / 2, p.stream));
-        }
-        p.yb_stale[n] = true;
+// ----------------------------------------------------------------------------
+//  plan from a .dnp image (runtime-only mode, src/dynasor_dnp.cpp:719-803):
+//  the saved slab(s), shard tables and schedule are used as they are; the
+//  device checks every index range, the per-shard counts, the shard order of
+//  the processing slab(s) and, on fiber-sorted NCopy copies, the row order.
+// ----------------------------------------------------------------------------
+__global__ void k_check_order(const uint32_t* __restrict__ idx, const Tile* __restrict__ tiles,
+                              int shift, const uint64_t* __restrict__ sbeg, int rows_sorted,
+                              int* __restrict__ err)
+{
+    const Tile tl = tiles[blockIdx.x];
+    for (uint32_t j = threadIdx.x; j < tl.count; j += blockDim.x) {
+        const uint64_t i = (uint64_t)tl.begin + j;
+        const uint32_t r = idx[i];
+        if ((r >> shift) != tl.shard) atomicOr(err, 0x400);
+        if (rows_sorted && i > sbeg[tl.shard] && idx[i - 1] > r) atomicOr(err, 0x800);
     }
-    DGPU_TRY(dev_alloc(p, (void**)&p.lambda, (size_t)p.Rp * sizeof(float)));
+}
+
+static int check_order(Plan& p, int n, const Slab& s, int rows_sorted) {
+    const uint32_t nt = (uint32_t)p.tiles_h[n].size();
+    if (nt == 0) return DGPU_OK;
+    uint64_t* sb = nullptr;
+    DGPU_TRY(dev_alloc(p, (void**)&sb, (size_t)p.K[n] * 8));
+    DGPU_CUDA(cudaMemcpyAsync(sb, p.sbeg[n].data(), (size_t)p.K[n] * 8, cudaMemcpyHostToDevice,
+                              p.stream));
+    DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
+    k_check_order<<<nt, 256, 0, p.stream>>>(s.idx[n], p.tiles_d[n], p.shift[n], sb, rows_sorted,
+                                             p.err_flag);
+    DGPU_CUDA(cudaGetLastError());
+    int err_h = 0;
+    DGPU_CUDA(cudaMemcpyAsync(&err_h, p.err_flag, sizeof(int), cudaMemcpyDeviceToHost, p.stream));
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    dev_free(sb);
+    p.device_bytes -= (size_t)p.K[n] * 8;
+    DGPU_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), p.stream));
+    if (err_h & 0x400) {
+        set_error("dnp: slab %s is not in mode-%d shard order", p.layout == DGPU_LAYOUT_NCOPY ?
+                  "copy" : "(PingPong)", n);
+        return DGPU_ERR_IO;
+    }
+    if (err_h & 0x800) {
+        set_error("dnp: NCopy copy %d is flagged fiber-sorted but its rows are not sorted", n);
+        return DGPU_ERR_IO;
+    }
+    return DGPU_OK;
+}
+
+int plan_build_dnp(Plan& p, const DnpImage& img, const dgpu_plan_opts& o) {
+    dgpu_plan_opts oo = o;
+    oo.threads = img.threads;
+    oo.layout = img.layout;
+    if (img.layout == DGPU_LAYOUT_NCOPY) {
+        // the copies decide: fiber-sorted DenseFiber copies, or none
+        bool any = false;
+        for (int k = 0; k < img.N; ++k) any = any || img.fiber_sorted[k];
+        oo.fiber = any ? 1 : 0;
+    }
+    DGPU_TRY(plan_init(p, img.N, img.nnz, img.dims, oo));
+    for (int n = 0; n < p.N; ++n) {
+        const uint32_t mn = img.mn[n];
+        if (mn == 0 || (mn & (mn - 1)) != 0) {
+            set_error("dnp: mode %d has %u rows per shard (not a power of two)", n, mn);
+            return DGPU_ERR_IO;
+        }
+        plan_mode_geometry(p, n, mn);
+        if (p.K[n] != img.K[n] || p.shift[n] != img.shift[n]) {
+            set_error("dnp: mode %d shard geometry (K %u, shift %d) does not match its size %u "
+                      "and %u rows per shard", n, img.K[n], img.shift[n], p.dims[n], mn);
+            return DGPU_ERR_IO;
+        }
+        if (img.kclass[n] > 2) {
+            set_error("dnp: mode %d kernel class %u unknown", n, img.kclass[n]);
+            return DGPU_ERR_IO;
+        }
+        p.afl[n] = img.afl[n];
+        p.kclass[n] = (int)img.kclass[n];
+        if (img.layout == DGPU_LAYOUT_NCOPY &&
+            (img.fiber_sorted[n] != 0) != (p.fiber && p.kclass[n] == 2)) {
+            set_error("dnp: NCopy copy %d fiber-sorted flag %d does not match its kernel class %d",
+                      n, (int)img.fiber_sorted[n], p.kclass[n]);
+            return DGPU_ERR_IO;
+        }
+    }
+    // shard tables: contiguous ranges covering the slab
+    p.sbeg = img.sbeg;
+    p.send = img.send;
+    p.count.assign(p.N, {});
+    for (int n = 0; n < p.N; ++n) {
+        if (p.sbeg[n].size() != p.K[n] || p.send[n].size() != p.K[n]) {
+            set_error("dnp: mode %d shard table size differs from %u shards", n, p.K[n]);
+            return DGPU_ERR_IO;
+        }
+        uint64_t c = 0;
+        p.count[n].resize(p.K[n]);
+        for (uint32_t s = 0; s < p.K[n]; ++s) {
+            if (p.sbeg[n][s] != c || p.send[n][s] < c) {
+                set_error("dnp: mode %d shard %u range [%llu,%llu) is not contiguous", n, s,
+                          (unsigned long long)p.sbeg[n][s], (unsigned long long)p.send[n][s]);
+                return DGPU_ERR_IO;
+            }
+            p.count[n][s] = p.send[n][s] - c;
+            c = p.send[n][s];
+        }
+        if (c != p.nnz) {
+            set_error("dnp: mode %d shard ranges cover %llu of %llu nonzeros", n,
+                      (unsigned long long)c, (unsigned long long)p.nnz);
+            return DGPU_ERR_IO;
+        }
+    }
+    // schedule: every non-empty shard exactly once, empty ones at most once
+    p.sched = img.sched;
+    for (int n = 0; n < p.N; ++n) {
+        std::vector<uint8_t> seen(p.K[n], 0);
+        if ((int)p.sched[n].size() != p.T) {
+            set_error("dnp: mode %d schedule has %zu thread lists, expected %d", n,
+                      p.sched[n].size(), p.T);
+            return DGPU_ERR_IO;
+        }
+        for (const auto& lst : p.sched[n])
+            for (uint32_t s : lst) {
+                if (s >= p.K[n] || seen[s]) {
+                    set_error("dnp: mode %d schedule names shard %u %s", n, s,
+                              s >= p.K[n] ? "out of range" : "twice");
+                    return DGPU_ERR_IO;
+                }
+                seen[s] = 1;
+            }
+        for (uint32_t s = 0; s < p.K[n]; ++s)
+            if (!seen[s] && p.count[n][s]) {
+                set_error("dnp: mode %d schedule omits non-empty shard %u", n, s);
+                return DGPU_ERR_IO;
+            }
+    }
+    DGPU_TRY(plan_alloc_slabs(p));
+    const int ncopies = (img.layout == DGPU_LAYOUT_NCOPY) ? p.N : 1;
+    for (int k = 0; k < ncopies; ++k) {
+        Slab& d = p.slab[k];
+        DGPU_CUDA(cudaMemcpyAsync(d.vals, img.vals[k].data(), p.nnz * sizeof(float),
+                                  cudaMemcpyHostToDevice, p.stream));
+        for (int m = 0; m < p.N; ++m)
+            DGPU_CUDA(cudaMemcpyAsync(d.idx[m], img.idx[k][m].data(), p.nnz * sizeof(uint32_t),
+                                      cudaMemcpyHostToDevice, p.stream));
+        // index ranges and shard counts of every copy
+        std::vector<std::vector<uint64_t>> cnt;
+        DGPU_TRY(device_shard_counts(p, d, cnt));
+        for (int n = 0; n < p.N; ++n)
+            if (cnt[n] != p.count[n]) {
+                set_error("dnp: %s %d holds shard counts of mode %d that differ from the shard "
+                          "table", ncopies > 1 ? "copy" : "slab", k, n);
+                return DGPU_ERR_IO;
+            }
+    }
+    DGPU_TRY(plan_tables(p));
+    if (img.layout == DGPU_LAYOUT_NCOPY) {
+        for (int k = 0; k < p.N; ++k) DGPU_TRY(check_order(p, k, p.slab[k], img.fiber_sorted[k]));
+    } else {
+        DGPU_TRY(check_order(p, 0, p.slab[0], 0));
+    }
+    p.cur = 0;
+    p.next_mode = 0;
+    DGPU_TRY(plan_factors(p));
     DGPU_TRY(sync_checked(p));
     return DGPU_OK;
 }

@@ -151,6 +151,51 @@ void dgpu_plan_opts_default(dgpu_plan_opts* opts);
 int  dgpu_plan_create(const dgpu_tensor_desc* tensor, const dgpu_plan_opts* opts,
                       dgpu_plan** out);
 int  dgpu_plan_destroy(dgpu_plan* plan);
+
+/* ---- processed-tensor files (.dnp, src/dynasor_dnp.cpp) ---------------- */
+/* layout_kind values of a .dnp header (src/dynasor_dnp.cpp:30-34) */
+#define DGPU_DNP_MORTON      0
+#define DGPU_DNP_NCOPY       1
+#define DGPU_DNP_PINGPONG    2
+#define DGPU_DNP_INPLACE     3
+
+typedef struct {
+    int       layout_kind;                      /* DGPU_DNP_*             */
+    int       num_modes;
+    uint64_t  nnz;
+    uint32_t  mode_size[DGPU_MAX_MODES];
+    int       num_threads;                      /* thread count the schedule
+                                                   was built for          */
+} dgpu_dnp_info;
+
+/* Header of a .dnp file; host only, no device needed.  Replaces
+ * load_dnp_header / load_dnp_num_threads / load_dnp_layout
+ * (include/dynasor_dnp.h:127-140).  DGPU_ERR_IO for a missing file, bad
+ * magic, version, value/index width, mode count, nnz or layout kind. */
+int  dgpu_dnp_peek(const char* path, dgpu_dnp_info* info);
+
+/* Plan from a .dnp file (runtime-only mode; replaces load_dnp_tensor,
+ * include/dynasor_dnp.h:149-151, plus build_flycoo's work).  The file's
+ * slab(s), shard tables and schedule are used as they are (no device sort);
+ * the device checks index ranges, per-shard counts, shard order and, on
+ * fiber-sorted NCopy copies, row order (DGPU_ERR_IO when one fails).
+ * opts->threads must equal the file's thread count (DGPU_ERR_ARG, as the
+ * reference rejects a mismatch); the file decides layout, rows per shard and
+ * kernel classes (opts->layout and ->mn_target are ignored; so is
+ * opts->fiber for NCopy files, whose copies say whether they are
+ * fiber-sorted).  PingPong and NCopy files only: Morton and InPlace files
+ * give DGPU_ERR_ARG. */
+int  dgpu_plan_create_from_dnp(const char* path, const dgpu_plan_opts* opts,
+                               dgpu_plan** plan);
+
+/* Write the plan as a .dnp file (replaces save_dnp_tensor,
+ * include/dynasor_dnp.h:121-123).  PingPong plans between sweeps (next mode
+ * 0; DGPU_ERR_ORDER otherwise), NCopy plans at any time.  A plan built from
+ * the same tensor with the same threads and layout writes the bytes the
+ * reference writes after build_flycoo (NCopy: fiber-sorted copies carry
+ * their CSR row pointers, as with --ncopy-csr-compact off).  Synchronises
+ * the plan stream. */
+int  dgpu_plan_save_dnp(const dgpu_plan* plan, const char* path);
 int  dgpu_plan_get_info(const dgpu_plan* plan, dgpu_plan_info* info);
 int  dgpu_plan_set_stream(dgpu_plan* plan, void* cuda_stream);
 int  dgpu_plan_sync(dgpu_plan* plan);

@@ -282,6 +282,10 @@ def _ref_lib():
                                 C.c_int, _f64p, _f32p, C.c_void_p, C.c_void_p]
         L.ref_spmttkrp_dynasor.restype = C.c_double
         L.ref_spmttkrp_dynasor.argtypes = [C.c_void_p]
+        L.ref_save_dnp.restype = C.c_int
+        L.ref_save_dnp.argtypes = [C.c_void_p, C.c_char_p]
+        L.ref_load_dnp.restype = C.c_void_p
+        L.ref_load_dnp.argtypes = [C.c_char_p, C.c_int, C.c_int]
         _rlib = L
     return _rlib
 
@@ -308,10 +312,35 @@ class Reference:
             self.L.ref_destroy(self.h)
             self.h = None
 
+    @classmethod
+    def from_dnp(cls, path, threads, quiet=True):
+        """A tensor loaded by the reference's .dnp reader (load_dnp_tensor,
+        src/dynasor_dnp.cpp:719-803); None when the reader rejects it."""
+        import struct
+        with open(path, "rb") as f:
+            head = f.read(4 + 5 * 4 + 8 + 8 * 4)
+        N, nnz = struct.unpack_from("<I", head, 20)[0], struct.unpack_from("<Q", head, 24)[0]
+        dims = np.array(struct.unpack_from("<8I", head, 32)[:N], np.uint32)
+        self = cls.__new__(cls)
+        self.L = _ref_lib()
+        self.h = self.L.ref_load_dnp(str(path).encode(), int(threads), 1 if quiet else 0)
+        if not self.h:
+            return None
+        self.N, self.dims, self.nnz, self.Rp = N, dims, int(nnz), None
+        self._plan_facts(threads)
+        return self
+
+    def save_dnp(self, path):
+        """save_dnp_tensor on the built tensor (src/dynasor_dnp.cpp:639-700)."""
+        return self.L.ref_save_dnp(self.h, str(path).encode()) == 0
+
     def build(self, threads, layout="pingpong"):
-        self.T = int(threads)
-        got = self.L.ref_build_flycoo(self.h, self.T, layout.encode())
+        got = self.L.ref_build_flycoo(self.h, int(threads), layout.encode())
         assert got == self.LAYOUTS[layout], (got, layout)
+        self._plan_facts(threads)
+
+    def _plan_facts(self, threads):
+        self.T = int(threads)
         self.shift = np.zeros(self.N, np.int32)
         self.K = np.zeros(self.N, np.uint32)
         self.kclass = np.zeros(self.N, np.int32)

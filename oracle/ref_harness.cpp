@@ -10,6 +10,7 @@
 //    * SpmttkrpSweep::process  (src/dynasor.cpp:352-539)
 //    * spmttkrp_reference      (src/dynasor_reference.cpp:18-50)
 //    * cpals                   (src/dynasor_cpals.cpp:120-396)
+//    * save_dnp_tensor / load_dnp_tensor (src/dynasor_dnp.cpp:639-803)
 //
 //  and to read back the FLYCOO plan tables and the SoA slab after each
 //  process(n), which is what the bit-exact remap parity tests compare.
@@ -18,6 +19,7 @@
 // ============================================================================
 #include "dynasor_common.h"
 #include "dynasor_cpals.h"
+#include "dynasor_dnp.h"
 #include "dynasor_linalg.h"
 
 #include <cstdint>
@@ -285,6 +287,38 @@ int ref_simd_width_hint(void) {
 #else
     return 4;
 #endif
+}
+
+// The reference's .dnp writer on the built tensor; 0 on success.
+int ref_save_dnp(void* hp, const char* path)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    Quiet q(h->quiet);
+    return save_dnp_tensor(path, h->T, h->threads) ? 0 : -1;
+}
+
+// A tensor loaded by the reference's .dnp reader (runtime-only mode), or
+// null when the reader rejects the file.
+void* ref_load_dnp(const char* path, int threads, int quiet)
+{
+    auto* h = new RefHandle();
+    h->quiet = quiet != 0;
+    h->threads = threads;
+#ifdef _OPENMP
+    omp_set_num_threads(threads);
+#endif
+    bool ok;
+    {
+        Quiet q(h->quiet);
+        ok = load_dnp_tensor(path, h->T, threads);
+    }
+    if (!ok) { delete h; return nullptr; }
+    // The reference's PingPong loader (load_soa_slab, src/dynasor_dnp.cpp:
+    // 497-504) materialises only the primary slab; its first remap then
+    // writes through the unallocated scratch slab.  Materialise it here, as
+    // build_flycoo does (src/dynasor_preprocess.cpp:2029).
+    if (h->T.layout == Layout::PingPong || h->T.layout == Layout::InPlace) h->T.ensure_scratch();
+    return h;
 }
 
 } // extern "C"
