@@ -55,7 +55,7 @@ METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 NCU_DRAM_BYTES_PER_NNZ = {
     "part_scatter": 29.49,     # k_chunk_scatter, all launches averaged
     "fiber_scatter": 29.49,
-    "mttkrp": 38.55,           # k_mttkrp_rowrun, 3 modes averaged
+    "mttkrp": 47.29,           # k_mttkrp_rowrun, 3 modes averaged
 }
 
 
