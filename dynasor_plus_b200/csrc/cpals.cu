@@ -31,6 +31,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <random>
 #include <memory>
 #include <thread>
@@ -661,8 +662,11 @@ int init_factors_host(Plan& p, uint64_t seed) {
     // threads (large factors take seconds to draw serially)
     std::vector<std::vector<float>> Y(p.N);
     std::vector<std::thread> th;
-    for (int n = 0; n < p.N; ++n)
-        th.emplace_back([&, n]() {
+    size_t total = 0;
+    for (int n = 0; n < p.N; ++n) total += (size_t)p.dims[n] * p.R;
+    const bool par = total >= (1u << 20);       // small factors: no thread start-up
+    for (int n = 0; n < p.N; ++n) {
+        auto draw = [&, n]() {
             uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
             z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
             z ^= z >> 27; z *= 0x94D049BB133111EBULL;
@@ -672,7 +676,10 @@ int init_factors_host(Plan& p, uint64_t seed) {
             Y[n].assign((size_t)p.dims[n] * p.Rp, 0.f);
             for (uint32_t i = 0; i < p.dims[n]; ++i)
                 for (int r = 0; r < p.R; ++r) Y[n][(size_t)i * p.Rp + r] = g(rng);
-        });
+        };
+        if (par) th.emplace_back(draw);
+        else draw();
+    }
     for (auto& t : th) t.join();
     for (int n = 0; n < p.N; ++n) {
         DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y[n].data(), Y[n].size() * sizeof(float),
@@ -716,13 +723,15 @@ struct CpSession {
     LaLayout L{};
     double tn2 = 0.0;
     bool jacobi = false;
-    std::vector<cudaEvent_t> ev;
-    std::vector<cudaEvent_t> fork, join;     // side-stream solve of each mode
-    double* fit_host = nullptr;              // pinned: the per-iteration graphs' D2H target
+    // kept on the plan across calls (created on first use)
+    std::vector<cudaEvent_t>& ev;            // iteration timing
+    std::vector<cudaEvent_t>& fork;          // side-stream solve of each mode
+    std::vector<cudaEvent_t>& join;
+    double*& fit_host;                       // pinned: the per-iteration graphs' D2H target
+    double*& st;                             // device loop: [it, fit_prev] + fit/residual histories
+    size_t& st_bytes;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int cur_after[2] = {0, 0};
-    double* st = nullptr;                    // device loop: [it, fit_prev] + fit/residual histories
-    size_t st_bytes = 0;
     double fit_prev = 0.0;
     int cur_start = 0;
     int it = 0;                              // next iteration index
@@ -735,14 +744,18 @@ struct CpSession {
     bool stale0[kMaxModes] = {};
 
     CpSession(Plan& pl, const dgpu_cp_options& op, dgpu_cp_result& r, double* fh)
-        : p(pl), o(op), res(r), fit_history(fh) {}
+        : p(pl), o(op), res(r), fit_history(fh), ev(pl.cp_ev), fork(pl.cp_fork), join(pl.cp_join),
+          fit_host(pl.cp_fit_host), st(pl.cp_st), st_bytes(pl.cp_st_bytes) {}
     ~CpSession() {
-        for (auto e : ev) if (e) cudaEventDestroy(e);
-        for (auto e : fork) if (e) cudaEventDestroy(e);
-        for (auto e : join) if (e) cudaEventDestroy(e);
-        if (fit_host) cudaFreeHost(fit_host);
         for (int k = 0; k < 2; ++k) if (exec[k]) cudaGraphExecDestroy(exec[k]);
-        if (st) { dev_free(st); p.device_bytes -= st_bytes; }
+    }
+
+    static int ensure_events(std::vector<cudaEvent_t>& v, size_t n, unsigned flags) {
+        if (v.size() == n) return DGPU_OK;
+        for (auto e : v) if (e) cudaEventDestroy(e);
+        v.assign(n, nullptr);
+        for (auto& e : v) DGPU_CUDA(cudaEventCreateWithFlags(&e, flags));
+        return DGPU_OK;
     }
 
     int setup() {
@@ -750,8 +763,12 @@ struct CpSession {
         DGPU_TRY(la_ensure(p, L));
         if (!o.use_init) DGPU_TRY(init_factors_host(p, o.seed));
         for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
-        const Slab& vs = (p.layout == DGPU_LAYOUT_NCOPY) ? p.slab[0] : p.slab[p.cur];
-        DGPU_TRY(cp_tensor_norm(p, vs.vals, &tn2));
+        // ||T||^2 of the plan's values, computed once per plan
+        if (p.cp_tnorm2 < 0.0) {
+            const Slab& vs = (p.layout == DGPU_LAYOUT_NCOPY) ? p.slab[0] : p.slab[p.cur];
+            DGPU_TRY(cp_tensor_norm(p, vs.vals, &p.cp_tnorm2));
+        }
+        tn2 = p.cp_tnorm2;
         res.tensor_norm = std::sqrt(tn2);
         if (o.verbose)
             std::printf("[cpals] modes=%d  rank=%d  padded=%d  nnz=%llu  ||T|| = %.6e  max_iters=%d  "
@@ -760,15 +777,12 @@ struct CpSession {
         jacobi = (o.kernel == DGPU_CP_JACOBI);
         // ev[0] iteration start, ev[1 + 2n] end of mode n's MTTKRP (Jacobi:
         // ev[1] ends all MTTKRPs), ev[2 + 2n] end of mode n's factor update
-        ev.assign(2 * p.N + 2, nullptr);
-        for (auto& e : ev) DGPU_CUDA(cudaEventCreate(&e));
-        fork.assign(p.N, nullptr);
-        join.assign(p.N, nullptr);
-        for (auto& e : fork) DGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        for (auto& e : join) DGPU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        DGPU_TRY(ensure_events(ev, 2 * (size_t)p.N + 2, cudaEventDefault));
+        DGPU_TRY(ensure_events(fork, p.N, cudaEventDisableTiming));
+        DGPU_TRY(ensure_events(join, p.N, cudaEventDisableTiming));
         if (!p.side_stream)
             DGPU_CUDA(cudaStreamCreateWithFlags(&p.side_stream, cudaStreamNonBlocking));
-        DGPU_CUDA(cudaMallocHost((void**)&fit_host, 4 * sizeof(double)));
+        if (!fit_host) DGPU_CUDA(cudaMallocHost((void**)&fit_host, 4 * sizeof(double)));
         graphs = o.graphs != 0 && !p.timing;
         cur_start = p.cur;
         done = o.max_iters <= 0;
@@ -918,14 +932,53 @@ struct CpSession {
 
     // Captures one iteration + the loop control into `body` (the WHILE
     // node's graph).  DGPU_ERR_CUDA: capture not possible (state restored).
-    int capture_body(cudaGraph_t body, cudaGraphConditionalHandle h) {
-        if (!st) {
-            st_bytes = (2 + 2 * (size_t)o.max_iters) * sizeof(double);
-            DGPU_TRY(dev_alloc(p, (void**)&st, st_bytes));
+    // The loop state array (reallocated only to grow; a cached loop graph
+    // that read the old one is dropped).
+    int ensure_state() {
+        const size_t need = (2 + 2 * (size_t)o.max_iters) * sizeof(double);
+        if (st_bytes >= need) return DGPU_OK;
+        if (p.cp_loop_exec) {
+            cudaGraphExecDestroy(p.cp_loop_exec);
+            p.cp_loop_exec = nullptr;
         }
+        if (st) {
+            dev_free(st);
+            p.device_bytes -= st_bytes;
+            st = nullptr;
+            st_bytes = 0;
+        }
+        DGPU_TRY(dev_alloc(p, (void**)&st, need));
+        st_bytes = need;
+        return DGPU_OK;
+    }
+    int write_state() {
         const double init[2] = {(double)it, fit_prev};
         DGPU_CUDA(cudaMemcpyAsync(st, init, sizeof(init), cudaMemcpyHostToDevice, p.stream));
         DGPU_CUDA(cudaStreamSynchronize(p.stream));
+        return DGPU_OK;
+    }
+
+    // What the captured loop body depends on: options, tensor norm, live
+    // slab at the loop start and the device buffers it reads and writes.
+    void loop_key(uint64_t (&k)[12]) const {
+        auto bits = [](double v) { uint64_t u; std::memcpy(&u, &v, 8); return u; };
+        k[0] = (uint64_t)o.kernel;
+        k[1] = (uint64_t)o.solve_fp64;
+        k[2] = bits(o.ridge);
+        k[3] = bits(o.tol);
+        k[4] = (uint64_t)o.max_iters;
+        k[5] = bits(tn2);
+        k[6] = (uint64_t)cur_start | ((uint64_t)p.layout << 8) | ((uint64_t)p.precision << 16);
+        k[7] = (uint64_t)(uintptr_t)p.la_work;
+        k[8] = (uint64_t)(uintptr_t)p.la_f32;
+        k[9] = (uint64_t)(uintptr_t)st;
+        k[10] = (uint64_t)(uintptr_t)p.lambda;
+        k[11] = (uint64_t)(uintptr_t)p.Y[0];
+    }
+
+    int capture_body(cudaGraph_t body, cudaGraphConditionalHandle h) {
+        DGPU_TRY(ensure_state());
+        DGPU_TRY(write_state());
         save_state();
         if (cudaStreamBeginCaptureToGraph(p.stream, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed) != cudaSuccess) {
@@ -1031,14 +1084,62 @@ int run_loops(std::vector<CpSession*>& ss, cudaStream_t launch) {
     return DGPU_OK;
 }
 
+// The device loop of one run, with its executable graph kept on the plan:
+// a later run with the same loop key relaunches it (after writing the loop
+// state) instead of capturing and instantiating it again.
+int run_loop_cached(CpSession& s) {
+    Plan& p = s.p;
+    uint64_t key[12];
+    DGPU_TRY(s.ensure_state());
+    s.loop_key(key);
+    if (!p.cp_loop_exec || std::memcmp(key, p.cp_loop_key, sizeof(key)) != 0) {
+        if (p.cp_loop_exec) {
+            cudaGraphExecDestroy(p.cp_loop_exec);
+            p.cp_loop_exec = nullptr;
+        }
+        cudaGraph_t outer = nullptr;
+        DGPU_CUDA(cudaGraphCreate(&outer, 0));
+        struct G { cudaGraph_t g; ~G() { if (g) cudaGraphDestroy(g); } } gg{outer};
+        cudaGraphConditionalHandle h;
+        DGPU_CUDA(cudaGraphConditionalHandleCreate(&h, outer, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        DGPU_CUDA(cudaGraphAddNode(&node, outer, nullptr, 0, &np));
+        const int rc = s.capture_body(np.conditional.phGraph_out[0], h);
+        if (rc == DGPU_ERR_CUDA) {
+            s.graphs = false;                    // iterate from the host
+            return DGPU_OK;
+        }
+        DGPU_TRY(rc);
+        if (cudaGraphInstantiate(&p.cp_loop_exec, outer, 0) != cudaSuccess) {
+            cudaGetLastError();
+            p.cp_loop_exec = nullptr;
+            s.restore_state();
+            s.graphs = false;
+            return DGPU_OK;
+        }
+        std::memcpy(p.cp_loop_key, key, sizeof(key));
+    } else {
+        DGPU_TRY(s.write_state());
+    }
+    DGPU_CUDA(cudaEventRecord(s.ev[0], p.stream));
+    DGPU_CUDA(cudaGraphLaunch(p.cp_loop_exec, p.stream));
+    DGPU_CUDA(cudaEventRecord(s.ev[1], p.stream));
+    DGPU_CUDA(cudaEventSynchronize(s.ev[1]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s.ev[0], s.ev[1]);
+    return s.finish_loop(ms);
+}
+
 int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fit_history) {
     CpSession s(p, o, res, fit_history);
     DGPU_TRY(s.setup());
     if (!s.done) DGPU_TRY(s.step_host());
-    if (s.loop_eligible()) {
-        std::vector<CpSession*> one{&s};
-        DGPU_TRY(run_loops(one, p.stream));
-    }
+    if (s.loop_eligible()) DGPU_TRY(run_loop_cached(s));
     while (!s.done) DGPU_TRY(s.step_host());
     s.finish();
     return DGPU_OK;

@@ -209,6 +209,17 @@ struct Plan {
     float*       la_f32 = nullptr;              // FP32 scratch (Grams etc.)
     size_t       la_f32_cap = 0;
     uint64_t     device_bytes = 0;
+    // CP-ALS state kept across cpals calls on this plan: the pinned fit
+    // buffer, the device loop's state array, timing / fork-join events, and
+    // the device-loop graph of the last run with the key it was captured for
+    // (options, norm, live slab and the buffers it reads)
+    double*      cp_fit_host = nullptr;         // pinned [4]
+    double*      cp_st = nullptr;               // device loop state
+    size_t       cp_st_bytes = 0;
+    std::vector<cudaEvent_t> cp_ev, cp_fork, cp_join;
+    cudaGraphExec_t cp_loop_exec = nullptr;
+    uint64_t     cp_loop_key[12] = {};
+    double       cp_tnorm2 = -1.0;              // ||T||^2 once computed (< 0: not yet)
 
     ~Plan();
 };

@@ -181,6 +181,12 @@ Plan::~Plan() {
     dev_free(lambda);
     dev_free(la_work);
     dev_free(la_f32);
+    if (cp_loop_exec) cudaGraphExecDestroy(cp_loop_exec);
+    dev_free(cp_st);
+    if (cp_fit_host) cudaFreeHost(cp_fit_host);
+    for (auto e : cp_ev) cudaEventDestroy(e);
+    for (auto e : cp_fork) cudaEventDestroy(e);
+    for (auto e : cp_join) cudaEventDestroy(e);
     if (copy_stream) { cudaStreamSynchronize(copy_stream); cudaStreamDestroy(copy_stream); }
     if (side_stream) { cudaStreamSynchronize(side_stream); cudaStreamDestroy(side_stream); }
     if (own_stream && stream) cudaStreamDestroy(stream);
