@@ -28,13 +28,14 @@ from ._lib import (CpOptions, CpResult, Coo, DgpuError, DnpInfo, PlanInfo, PlanO
 
 __all__ = ["Plan", "DgpuError", "cpals_batch", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
            "dnp_peek",
-           "spmttkrp_dynasor", "device_count", "LIB_PATH", "PINGPONG", "NCOPY", "AUTO"]
+           "spmttkrp_dynasor", "device_count", "LIB_PATH", "PINGPONG", "NCOPY", "MORTON", "AUTO"]
 
 PINGPONG = 0
 NCOPY = 1
-AUTO = 2  # NCopy when its slabs fit the device-memory budget, else PingPong
-LAYOUTS = {"pingpong": PINGPONG, "ncopy": NCOPY, "auto": AUTO}
-LAYOUT_NAMES = {PINGPONG: "pingpong", NCOPY: "ncopy"}
+MORTON = 4  # one sorted 64-bit interleaved key + value per nonzero (all-modes pass only)
+AUTO = 16  # NCopy when its slabs fit the device-memory budget, else PingPong
+LAYOUTS = {"pingpong": PINGPONG, "ncopy": NCOPY, "morton": MORTON, "auto": AUTO}
+LAYOUT_NAMES = {PINGPONG: "pingpong", NCOPY: "ncopy", MORTON: "morton"}
 PRECISIONS = {"fp32": 0, "bf16": 1}
 ACCUMS = {"auto": 0, "rowrun": 1, "private": 2}
 
@@ -63,7 +64,9 @@ class Plan:
     idx    : N uint32 arrays of 0-based indices
     threads: the reference worker count the plan is built for (--threads)
     rank   : R; factors are I_n x padded_rank(R) float32
-    layout : "pingpong" (device remap every mode), "ncopy", or "auto" (NCopy
+    layout : "pingpong" (device remap every mode), "ncopy", "morton" (one
+             sorted interleaved 64-bit key + value per nonzero; all-modes
+             pass, sweeps and Jacobi CP-ALS only), or "auto" (NCopy
              when N+1 slabs fit 70% of free device memory less a headroom of
              max(2 GiB, 25% of total), else PingPong; info()["layout"] tells)
     fiber  : fiber-sort DenseFiber modes (reference default) or not
@@ -140,6 +143,18 @@ class Plan:
         if stream is not None:
             self.set_stream(stream)
         return self
+
+    def morton(self, keys: bool = True):
+        """Morton layout state: (mask[N] uint64, bits[N] uint8, sorted keys
+        uint64[nnz], values float32[nnz]); keys/values None when keys=False."""
+        mask = np.zeros(self.N, np.uint64)
+        bits = np.zeros(self.N, np.uint8)
+        k = np.zeros(self.nnz, np.uint64) if keys else None
+        v = np.zeros(self.nnz, np.float32) if keys else None
+        check(lib().dgpu_plan_morton(self._h, mask.ctypes.data, bits.ctypes.data,
+                                     k.ctypes.data if keys else None,
+                                     v.ctypes.data if keys else None))
+        return mask, bits, k, v
 
     def save_dnp(self, path):
         """Write the plan as a .dnp file (save_dnp_tensor): PingPong plans

@@ -85,6 +85,7 @@ _SIGS = {
     "dgpu_dnp_peek": (C.c_int, [C.c_char_p, C.POINTER(DnpInfo)]),
     "dgpu_plan_create_from_dnp": (C.c_int, [C.c_char_p, C.POINTER(PlanOpts), C.POINTER(C.c_void_p)]),
     "dgpu_plan_save_dnp": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "dgpu_plan_morton": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dgpu_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "dgpu_plan_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dgpu_plan_sync": (C.c_int, [C.c_void_p]),

@@ -104,7 +104,7 @@ int dgpu_plan_create(const dgpu_tensor_desc* t, const dgpu_plan_opts* o, dgpu_pl
         set_error("dgpu_plan_create: rank %d outside [1,1024]", o->rank); return DGPU_ERR_ARG;
     }
     if (o->layout != DGPU_LAYOUT_PINGPONG && o->layout != DGPU_LAYOUT_NCOPY &&
-        o->layout != DGPU_LAYOUT_AUTO) {
+        o->layout != DGPU_LAYOUT_MORTON && o->layout != DGPU_LAYOUT_AUTO) {
         set_error("dgpu_plan_create: unknown layout %d", o->layout); return DGPU_ERR_ARG;
     }
     if (o->precision != DGPU_PREC_FP32 && o->precision != DGPU_PREC_BF16) {
@@ -295,6 +295,11 @@ int dgpu_mttkrp_mode(dgpu_plan* plan, int n) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
     MODE_GUARD(p, n);
+    if (p->layout == DGPU_LAYOUT_MORTON) {
+        set_error("dgpu_mttkrp_mode: a Morton plan runs the all-modes pass only "
+                  "(dgpu_mttkrp_all_modes / dgpu_mttkrp_sweep)");
+        return DGPU_ERR_ARG;
+    }
     if (p->layout == DGPU_LAYOUT_NCOPY) return mode_ncopy(*p, n);
     return mode_pingpong(*p, n);
 }
@@ -302,6 +307,9 @@ int dgpu_mttkrp_mode(dgpu_plan* plan, int n) {
 int dgpu_mttkrp_sweep(dgpu_plan* plan) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
+    // a sweep without factor updates computes every mode from the same
+    // factors: on the Morton layout that is one all-modes pass
+    if (p->layout == DGPU_LAYOUT_MORTON) return launch_mttkrp_all_modes(*p);
     for (int n = 0; n < p->N; ++n) {
         const int rc = (p->layout == DGPU_LAYOUT_NCOPY) ? mode_ncopy(*p, n) : mode_pingpong(*p, n);
         if (rc != DGPU_OK) return rc;
@@ -320,6 +328,31 @@ int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y, float* const*
         set_error("dgpu_mttkrp_sweep_host: the slab is ordered for mode %d, a sweep starts at 0",
                   p->next_mode);
         return DGPU_ERR_ORDER;
+    }
+    if (p->layout == DGPU_LAYOUT_MORTON) {
+        // one all-modes pass between the uploads and the downloads
+        cudaEvent_t a = nullptr, b = nullptr;
+        DGPU_CUDA(cudaEventCreate(&a));
+        DGPU_CUDA(cudaEventCreate(&b));
+        struct E { cudaEvent_t& a; cudaEvent_t& b; ~E() { cudaEventDestroy(a); cudaEventDestroy(b); } } eg{a, b};
+        for (int w = 0; w < p->N; ++w) {
+            DGPU_CUDA(cudaMemcpyAsync(p->Y[w], Y[w], (size_t)p->dims[w] * p->Rp * sizeof(float),
+                                      cudaMemcpyHostToDevice, p->stream));
+            p->yb_stale[w] = true;
+        }
+        DGPU_CUDA(cudaEventRecord(a, p->stream));
+        DGPU_TRY(launch_mttkrp_all_modes(*p));
+        DGPU_CUDA(cudaEventRecord(b, p->stream));
+        for (int n = 0; n < p->N; ++n)
+            DGPU_CUDA(cudaMemcpyAsync(Yhat[n], p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
+                                      cudaMemcpyDeviceToHost, p->stream));
+        DGPU_TRY(sync_checked(*p));
+        if (secs) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            *secs = ms * 1e-3;
+        }
+        return DGPU_OK;
     }
     // Transfers overlap the mode passes on a second stream: the factors mode 0
     // gathers go first, Y[0] (first needed by mode 1) streams in while mode 0
@@ -387,6 +420,25 @@ int dgpu_download_slab(dgpu_plan* plan, float* vals, uint32_t* const* idx) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
     if (!vals || !idx) { set_error("dgpu_download_slab: null"); return DGPU_ERR_ARG; }
+    for (int n = 0; n < p->N; ++n)
+        if (!idx[n]) { set_error("dgpu_download_slab: idx[%d] null", n); return DGPU_ERR_ARG; }
+    if (p->layout == DGPU_LAYOUT_MORTON) {
+        // key order, indices decoded on the host (pext by each mode's mask)
+        std::vector<uint64_t> keys(p->nnz);
+        DGPU_CUDA(cudaMemcpyAsync(keys.data(), p->mkeys, p->nnz * sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, p->stream));
+        DGPU_CUDA(cudaMemcpyAsync(vals, p->mvals, p->nnz * sizeof(float), cudaMemcpyDeviceToHost,
+                                  p->stream));
+        DGPU_TRY(sync_checked(*p));
+        const MortonDec d = morton_decoder(*p);
+        for (int n = 0; n < p->N; ++n)
+            for (uint64_t i = 0; i < p->nnz; ++i) {
+                uint32_t x = 0;
+                for (int j = 0; j < d.bits[n]; ++j) x |= (uint32_t)((keys[i] >> d.pos[n][j]) & 1u) << j;
+                idx[n][i] = x;
+            }
+        return DGPU_OK;
+    }
     const Slab& s = (p->layout == DGPU_LAYOUT_NCOPY) ? p->slab[p->next_mode] : p->slab[p->cur];
     DGPU_CUDA(cudaMemcpyAsync(vals, s.vals, p->nnz * sizeof(float), cudaMemcpyDeviceToHost, p->stream));
     for (int n = 0; n < p->N; ++n) {
@@ -394,6 +446,26 @@ int dgpu_download_slab(dgpu_plan* plan, float* vals, uint32_t* const* idx) {
         DGPU_CUDA(cudaMemcpyAsync(idx[n], s.idx[n], p->nnz * sizeof(uint32_t),
                                   cudaMemcpyDeviceToHost, p->stream));
     }
+    DGPU_TRY(sync_checked(*p));
+    return DGPU_OK;
+}
+
+int dgpu_plan_morton(dgpu_plan* plan, uint64_t* mask, uint8_t* bits, uint64_t* keys, float* vals) {
+    Plan* p = reinterpret_cast<Plan*>(plan);
+    API_GUARD(p);
+    if (p->layout != DGPU_LAYOUT_MORTON) {
+        set_error("dgpu_plan_morton: plan layout is not Morton"); return DGPU_ERR_NOT_BUILT;
+    }
+    for (int n = 0; n < p->N; ++n) {
+        if (mask) mask[n] = p->mmask[n];
+        if (bits) bits[n] = p->mbits[n];
+    }
+    if (keys)
+        DGPU_CUDA(cudaMemcpyAsync(keys, p->mkeys, p->nnz * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                  p->stream));
+    if (vals)
+        DGPU_CUDA(cudaMemcpyAsync(vals, p->mvals, p->nnz * sizeof(float), cudaMemcpyDeviceToHost,
+                                  p->stream));
     DGPU_TRY(sync_checked(*p));
     return DGPU_OK;
 }
@@ -467,6 +539,10 @@ int dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* 
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
     if (!opt || !res) { set_error("dgpu_cpals_multistart: null argument"); return DGPU_ERR_ARG; }
+    if (p->layout == DGPU_LAYOUT_MORTON) {
+        set_error("dgpu_cpals_multistart: runs on the PingPong and NCopy layouts");
+        return DGPU_ERR_ARG;
+    }
     if (opt->max_iters < 0) { set_error("dgpu_cpals_multistart: max_iters < 0"); return DGPU_ERR_ARG; }
     if (restarts < 1 || p->R % restarts != 0) {
         set_error("dgpu_cpals_multistart: the plan rank %d is not a multiple of %d restarts", p->R,

@@ -41,7 +41,6 @@ namespace dgpu {
 
 int mode_pingpong(Plan& p, int n);
 int mode_ncopy(Plan& p, int n);
-int launch_mttkrp_all_modes(Plan& p, const Slab& in);
 
 namespace {
 
@@ -764,17 +763,18 @@ struct CpSession {
         if (!o.use_init) DGPU_TRY(init_factors_host(p, o.seed));
         for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
         // ||T||^2 of the plan's values, computed once per plan
-        if (p.cp_tnorm2 < 0.0) {
-            const Slab& vs = (p.layout == DGPU_LAYOUT_NCOPY) ? p.slab[0] : p.slab[p.cur];
-            DGPU_TRY(cp_tensor_norm(p, vs.vals, &p.cp_tnorm2));
-        }
+        if (p.cp_tnorm2 < 0.0) DGPU_TRY(cp_tensor_norm(p, live_vals(p), &p.cp_tnorm2));
         tn2 = p.cp_tnorm2;
         res.tensor_norm = std::sqrt(tn2);
         if (o.verbose)
             std::printf("[cpals] modes=%d  rank=%d  padded=%d  nnz=%llu  ||T|| = %.6e  max_iters=%d  "
                         "tol=%.1e  seed=%llu\n", p.N, p.R, p.Rp, (unsigned long long)p.nnz,
                         res.tensor_norm, o.max_iters, o.tol, (unsigned long long)o.seed);
-        jacobi = (o.kernel == DGPU_CP_JACOBI);
+        // the Morton layout has only the all-modes pass: Gauss-Seidel runs
+        // as Jacobi there, as the reference does (src/dynasor_cpals.cpp:232-240)
+        jacobi = (o.kernel == DGPU_CP_JACOBI) || p.layout == DGPU_LAYOUT_MORTON;
+        if (p.layout == DGPU_LAYOUT_MORTON && o.kernel != DGPU_CP_JACOBI && o.verbose)
+            std::printf("[cpals] WARN: Morton layout has no Gauss-Seidel driver; running Jacobi\n");
         // ev[0] iteration start, ev[1 + 2n] end of mode n's MTTKRP (Jacobi:
         // ev[1] ends all MTTKRPs), ev[2 + 2n] end of mode n's factor update
         DGPU_TRY(ensure_events(ev, 2 * (size_t)p.N + 2, cudaEventDefault));
@@ -820,7 +820,9 @@ struct CpSession {
         // pass but with a vector atomic per nonzero and mode, which on the
         // 4-mode, 200M-nonzero, rank-64 tensor ran at 3.9 iterations/s against
         // 18.6 for the mode passes.
-        if (jacobi)
+        if (jacobi && p.layout == DGPU_LAYOUT_MORTON)
+            DGPU_TRY(launch_mttkrp_all_modes(p));
+        else if (jacobi)
             for (int n = 0; n < p.N; ++n)
                 DGPU_TRY(p.layout == DGPU_LAYOUT_NCOPY ? mode_ncopy(p, n) : mode_pingpong(p, n));
         for (int n = 0; n < p.N; ++n) {
@@ -1219,8 +1221,7 @@ k_grad_rows(const float* __restrict__ Y, const float* __restrict__ Yhat, uint32_
 int cpopt_gradient(Plan& p, float* const* grad_host) {
     LaLayout L{};
     DGPU_TRY(la_ensure(p, L));
-    const Slab& in = (p.layout == DGPU_LAYOUT_NCOPY) ? p.slab[0] : p.slab[p.cur];
-    DGPU_TRY(launch_mttkrp_all_modes(p, in));
+    DGPU_TRY(launch_mttkrp_all_modes(p));
     for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
     float* g = nullptr;
     size_t gmax = 0;

@@ -220,6 +220,12 @@ struct Plan {
     cudaGraphExec_t cp_loop_exec = nullptr;
     uint64_t     cp_loop_key[12] = {};
     double       cp_tnorm2 = -1.0;              // ||T||^2 once computed (< 0: not yet)
+    // Morton layout: sorted keys and their values (the slabs are freed once
+    // they are built), per-mode masks and bit counts
+    uint64_t*    mkeys = nullptr;
+    float*       mvals = nullptr;
+    uint64_t     mmask[kMaxModes] = {};
+    uint8_t      mbits[kMaxModes] = {};
 
     ~Plan();
 };
@@ -240,6 +246,28 @@ int timing_collect(Plan& p);
 // waits that gave up, out-of-range keys); a raised flag is cleared and
 // reported as DGPU_ERR_DEVICE.
 int sync_checked(Plan& p);
+
+// ---- Morton layout (morton.cu) -------------------------------------------
+// Key bit positions of each mode's index bits, LSB first: decoding is pext
+// of the key by the mode's mask, encoding pdep (src/dynasor_morton.cpp:43-81).
+struct MortonDec {
+    uint8_t pos[kMaxModes][32];
+    uint8_t bits[kMaxModes];
+};
+// The reference's bit plan (src/dynasor_morton.cpp:99-134): b_n =
+// ceil(log2 I_n) (>= 1), bits handed out LSB-first round-robin over the
+// modes that still need bits.  False when sum b_n > 64.
+bool morton_plan(int N, const uint32_t* dims, uint64_t* mask, uint8_t* bits);
+MortonDec morton_decoder(const Plan& p);
+// Morton keys from slab[src] (COO in any order), sorted, into p.mkeys /
+// p.mvals; frees the slabs.
+int morton_build(Plan& p, int src);
+// p.mkeys / p.mvals already hold keys and values (e.g. read from a file):
+// check every key (decodes within range, re-encodes to itself, ascending)
+// and decode them into slab `dst` (vals + indices).
+int morton_check_decode(Plan& p, int dst);
+// Releases every slab of the plan (Morton plans keep keys and values only).
+void free_slabs(Plan& p);
 
 // ---- .dnp processed-tensor image (src/dynasor_dnp.cpp) ---------------------
 // Host copy of everything one .dnp file holds for the PingPong and NCopy
@@ -269,6 +297,10 @@ struct DnpImage {
     std::vector<float> vals[kMaxModes];                       // [copy][nnz]
     std::vector<uint32_t> idx[kMaxModes][kMaxModes];          // [copy][mode][nnz]
     std::vector<uint64_t> rowptr[kMaxModes];                  // [copy][I_k + 1] when csr[k]
+    uint64_t mmask[kMaxModes] = {};                           // Morton files
+    uint8_t  mbits[kMaxModes] = {};
+    std::vector<uint64_t> mkeys;
+    std::vector<float> mvals;
 };
 // A plan that uses the image's slabs, shard tables and schedule as they are.
 int plan_build_dnp(Plan& p, const DnpImage& img, const dgpu_plan_opts& o);
@@ -313,14 +345,17 @@ int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first,
 
 // MTTKRP of mode n over the tiles of the slab `in` into p.Yhat[n].
 int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles);
-int launch_mttkrp_all_modes(Plan& p, const Slab& in);
+// All-modes pass over the plan's live nonzeros (SoA slab or Morton keys).
+int launch_mttkrp_all_modes(Plan& p);
+// Values array of the live nonzeros (any order).
+const float* live_vals(const Plan& p);
 
 // FP32 -> BF16 factor mirror.
 int launch_to_bf16(Plan& p, int n);
 
 // Dense CP-ALS pieces.
 int cp_tensor_norm(Plan& p, const float* vals, double* out);
-int launch_model_values(Plan& p, const Slab& in, float* out);
+int launch_model_values(Plan& p, float* out);
 int cpopt_gradient(Plan& p, float* const* grad_host);
 
 }  // namespace dgpu

@@ -270,16 +270,17 @@ int dnp_read(const char* path, int threads, bool header_only, DnpImage& img, uin
     for (int n = 0; n < DGPU_MAX_MODES; ++n) img.dims[n] = n < img.N ? h.dims[n] : 0u;
     img.threads = (int)h.threads;
     img.tnorm_sq = h.tnorm_sq;
-    img.layout = h.kind == kKindNCopy ? DGPU_LAYOUT_NCOPY : DGPU_LAYOUT_PINGPONG;
+    img.layout = h.kind == kKindNCopy ? DGPU_LAYOUT_NCOPY
+               : h.kind == kKindMorton ? DGPU_LAYOUT_MORTON : DGPU_LAYOUT_PINGPONG;
     if (header_only) return DGPU_OK;
     if (threads > 0 && (int)h.threads != threads) {
         set_error("dnp: %s was saved with %u threads but %d were requested; the schedule and "
                   "cursors are specific to the thread count", path, h.threads, threads);
         return DGPU_ERR_ARG;
     }
-    if (h.kind != kKindPingPong && h.kind != kKindNCopy) {
-        set_error("dnp: %s holds the %s layout; this engine reads PingPong and NCopy files", path,
-                  kind_name(h.kind));
+    if (h.kind == kKindInPlace) {
+        set_error("dnp: %s holds the %s layout; this engine reads PingPong, NCopy and Morton "
+                  "files", path, kind_name(h.kind));
         return DGPU_ERR_ARG;
     }
     if (img.N < 2) {
@@ -290,6 +291,30 @@ int dnp_read(const char* path, int threads, bool header_only, DnpImage& img, uin
         set_error("dnp: %s: nnz %llu exceeds the 32-bit slab positions", path,
                   (unsigned long long)img.nnz);
         return DGPU_ERR_ARG;
+    }
+    if (h.kind == kKindMorton) {
+        // mask[8] (u64), bits[8] (u8; 8 bytes, so no padding), keys, values
+        // (src/dynasor_dnp.cpp:203-264)
+        r.bytes(img.mmask, sizeof(img.mmask));
+        r.bytes(img.mbits, sizeof(img.mbits));
+        const long here = std::ftell(f.get());
+        std::fseek(f.get(), 0, SEEK_END);
+        const long end = std::ftell(f.get());
+        std::fseek(f.get(), here, SEEK_SET);
+        const uint64_t need = img.nnz * 12ull;
+        if (!r.ok || here < 0 || end < here || (uint64_t)(end - here) < need) {
+            set_error("dnp: %s (Morton) body truncated", path);
+            return DGPU_ERR_IO;
+        }
+        img.mkeys.resize(img.nnz);
+        img.mvals.resize(img.nnz);
+        r.bytes(img.mkeys.data(), img.nnz * 8);
+        r.bytes(img.mvals.data(), img.nnz * 4);
+        if (!r.ok) {
+            set_error("dnp: %s (Morton) body truncated", path);
+            return DGPU_ERR_IO;
+        }
+        return DGPU_OK;
     }
     int rc = read_flycoo(r, img);
     if (rc != DGPU_OK) {
@@ -339,7 +364,8 @@ int dnp_write(const char* path, const DnpImage& img) {
     }
     Writer w{f.get()};
     const int N = img.N;
-    const uint32_t kind = img.layout == DGPU_LAYOUT_NCOPY ? kKindNCopy : kKindPingPong;
+    const uint32_t kind = img.layout == DGPU_LAYOUT_NCOPY ? kKindNCopy
+                        : img.layout == DGPU_LAYOUT_MORTON ? kKindMorton : kKindPingPong;
     w.bytes(kMagic, 4);
     w.put(kVersion);
     w.put((uint32_t)4);
@@ -352,6 +378,20 @@ int dnp_write(const char* path, const DnpImage& img) {
     w.put(img.tnorm_sq);
     const uint32_t reserved[14] = {};
     w.bytes(reserved, sizeof(reserved));
+    if (kind == kKindMorton) {
+        w.bytes(img.mmask, sizeof(img.mmask));
+        w.bytes(img.mbits, sizeof(img.mbits));
+        w.bytes(img.mkeys.data(), img.nnz * 8);
+        w.bytes(img.mvals.data(), img.nnz * 4);
+        const bool ok = w.ok;
+        f.reset();
+        if (!ok) {
+            std::remove(path);
+            set_error("dnp: I/O failure writing '%s'", path);
+            return DGPU_ERR_IO;
+        }
+        return DGPU_OK;
+    }
 
     uint32_t spm[DGPU_MAX_MODES] = {}, mn[DGPU_MAX_MODES] = {}, kcls[DGPU_MAX_MODES] = {};
     int32_t shft[DGPU_MAX_MODES] = {};
@@ -496,6 +536,19 @@ int plan_to_dnp(Plan& p, DnpImage& img) {
     for (int n = 0; n < DGPU_MAX_MODES; ++n) img.dims[n] = n < N ? p.dims[n] : 0u;
     img.threads = p.T;
     img.tnorm_sq = 0.0;             // in-core tensors carry no cached norm
+    if (p.layout == DGPU_LAYOUT_MORTON) {
+        for (int n = 0; n < N; ++n) {
+            img.mmask[n] = p.mmask[n];
+            img.mbits[n] = p.mbits[n];
+        }
+        img.mkeys.resize(p.nnz);
+        img.mvals.resize(p.nnz);
+        DGPU_CUDA(cudaMemcpyAsync(img.mkeys.data(), p.mkeys, p.nnz * 8, cudaMemcpyDeviceToHost,
+                                  p.stream));
+        DGPU_CUDA(cudaMemcpyAsync(img.mvals.data(), p.mvals, p.nnz * 4, cudaMemcpyDeviceToHost,
+                                  p.stream));
+        return sync_checked(p);
+    }
     img.shard_size = kShardSize;
     img.inplace_mode = 0;
     for (int n = 0; n < N; ++n) {

@@ -28,9 +28,38 @@ struct FacPtrs32 {
     const float* Y[kMaxModes];
 };
 
-template <int N, int G, int V>
+// Where a nonzero's value and indices come from: the SoA slab, or a Morton
+// key decoded in registers (pext of the key by each mode's mask,
+// src/dynasor_morton.cpp:466-470).
+struct SoaSrc {
+    SlabPtrs s;
+    template <int N>
+    __device__ __forceinline__ float load(uint64_t i, uint32_t (&id)[N]) const {
+#pragma unroll
+        for (int w = 0; w < N; ++w) id[w] = __ldg(s.idx[w] + i);
+        return __ldg(s.vals + i);
+    }
+};
+struct MortonSrc {
+    const uint64_t* keys;
+    const float*    vals;
+    MortonDec       d;
+    template <int N>
+    __device__ __forceinline__ float load(uint64_t i, uint32_t (&id)[N]) const {
+        const uint64_t k = __ldg(keys + i);
+#pragma unroll
+        for (int w = 0; w < N; ++w) {
+            uint32_t x = 0;
+            for (int j = 0; j < d.bits[w]; ++j) x |= (uint32_t)((k >> d.pos[w][j]) & 1u) << j;
+            id[w] = x;
+        }
+        return __ldg(vals + i);
+    }
+};
+
+template <int N, int G, int V, class Src>
 __global__ void __launch_bounds__(kThreads)
-k_mttkrp_all(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_constant__ FacPtrs32 F, float* Yh0, float* Yh1, float* Yh2, float* Yh3, float* Yh4, float* Yh5, float* Yh6,
+k_mttkrp_all(const __grid_constant__ Src in, uint64_t nnz, const __grid_constant__ FacPtrs32 F, float* Yh0, float* Yh1, float* Yh2, float* Yh3, float* Yh4, float* Yh5, float* Yh6,
              float* Yh7, int Rp)
 {
     float* Yh[8] = {Yh0, Yh1, Yh2, Yh3, Yh4, Yh5, Yh6, Yh7};
@@ -38,10 +67,8 @@ k_mttkrp_all(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_con
     const int C4 = Rp >> 2;
     const uint64_t groups = (uint64_t)gridDim.x * (kThreads / G);
     for (uint64_t i = (uint64_t)blockIdx.x * (kThreads / G) + threadIdx.x / G; i < nnz; i += groups) {
-        const float v = __ldg(in.vals + i);
         uint32_t id[N];
-#pragma unroll
-        for (int w = 0; w < N; ++w) id[w] = __ldg(in.idx[w] + i);
+        const float v = in.template load<N>(i, id);
 #pragma unroll
         for (int q = 0; q < V; ++q) {
             const int c4 = gl + q * G;
@@ -73,9 +100,9 @@ k_mttkrp_all(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_con
 }
 
 // model[i] = sum_r prod_w Y[w][i_w, r]  (one lane group per nonzero)
-template <int N, int G, int V>
+template <int N, int G, int V, class Src>
 __global__ void __launch_bounds__(kThreads)
-k_model_values(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_constant__ FacPtrs32 F, int Rp, float* __restrict__ out)
+k_model_values(const __grid_constant__ Src in, uint64_t nnz, const __grid_constant__ FacPtrs32 F, int Rp, float* __restrict__ out)
 {
     const int gl = threadIdx.x % G;
     const int C4 = Rp >> 2;
@@ -90,8 +117,7 @@ k_model_values(const __grid_constant__ SlabPtrs in, uint64_t nnz, const __grid_c
         float s = 0.f;
         if (ok) {
             uint32_t id[N];
-#pragma unroll
-            for (int w = 0; w < N; ++w) id[w] = __ldg(in.idx[w] + i);
+            in.template load<N>(i, id);
 #pragma unroll
             for (int q = 0; q < V; ++q) {
                 const int c4 = gl + q * G;
@@ -117,16 +143,15 @@ unsigned grid_groups(uint64_t nnz, int G) {
                                                              148ull * 16));
 }
 
-template <int N>
-int all_modes_n(Plan& p, const Slab& in) {
+template <int N, class Src>
+int all_modes_n(Plan& p, const Src& sp) {
     FacPtrs32 F{};
     for (int w = 0; w < N; ++w) F.Y[w] = p.Y[w];
     float* Yh[8] = {nullptr};
     for (int w = 0; w < N; ++w) Yh[w] = p.Yhat[w];
     const int C4 = p.Rp / 4;
-    const SlabPtrs sp = slab_in(in, p.N);
 #define LAUNCH(G, V)                                                                        \
-    k_mttkrp_all<N, G, V><<<grid_groups(p.nnz, G), kThreads, 0, p.stream>>>(               \
+    k_mttkrp_all<N, G, V, Src><<<grid_groups(p.nnz, G), kThreads, 0, p.stream>>>(          \
         sp, p.nnz, F, Yh[0], Yh[1], Yh[2], Yh[3], Yh[4], Yh[5], Yh[6], Yh[7], p.Rp)
     if (C4 == 4) LAUNCH(4, 1);
     else if (C4 == 8) LAUNCH(8, 1);
@@ -141,14 +166,13 @@ int all_modes_n(Plan& p, const Slab& in) {
     return DGPU_OK;
 }
 
-template <int N>
-int model_values_n(Plan& p, const Slab& in, float* out) {
+template <int N, class Src>
+int model_values_n(Plan& p, const Src& sp, float* out) {
     FacPtrs32 F{};
     for (int w = 0; w < N; ++w) F.Y[w] = p.Y[w];
     const int C4 = p.Rp / 4;
-    const SlabPtrs sp = slab_in(in, p.N);
 #define LAUNCH(G, V) \
-    k_model_values<N, G, V><<<grid_groups(p.nnz, G), kThreads, 0, p.stream>>>(sp, p.nnz, F, p.Rp, out)
+    k_model_values<N, G, V, Src><<<grid_groups(p.nnz, G), kThreads, 0, p.stream>>>(sp, p.nnz, F, p.Rp, out)
     if (C4 == 4) LAUNCH(4, 1);
     else if (C4 == 8) LAUNCH(8, 1);
     else if (C4 == 16) LAUNCH(16, 1);
@@ -182,14 +206,28 @@ const Slab& live_slab(const Plan& p) {
 
 }  // namespace
 
-int launch_mttkrp_all_modes(Plan& p, const Slab& in) {
-    for (int n = 0; n < p.N; ++n)
-        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, (size_t)p.dims[n] * p.Rp * sizeof(float), p.stream));
-    return by_modes(p.N, [&](auto NC) { return all_modes_n<decltype(NC)::value>(p, in); });
+const float* live_vals(const Plan& p) {
+    return p.layout == DGPU_LAYOUT_MORTON ? p.mvals : live_slab(p).vals;
 }
 
-int launch_model_values(Plan& p, const Slab& in, float* out) {
-    return by_modes(p.N, [&](auto NC) { return model_values_n<decltype(NC)::value>(p, in, out); });
+int launch_mttkrp_all_modes(Plan& p) {
+    for (int n = 0; n < p.N; ++n)
+        DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, (size_t)p.dims[n] * p.Rp * sizeof(float), p.stream));
+    if (p.layout == DGPU_LAYOUT_MORTON) {
+        const MortonSrc src{p.mkeys, p.mvals, morton_decoder(p)};
+        return by_modes(p.N, [&](auto NC) { return all_modes_n<decltype(NC)::value>(p, src); });
+    }
+    const SoaSrc src{slab_in(live_slab(p), p.N)};
+    return by_modes(p.N, [&](auto NC) { return all_modes_n<decltype(NC)::value>(p, src); });
+}
+
+int launch_model_values(Plan& p, float* out) {
+    if (p.layout == DGPU_LAYOUT_MORTON) {
+        const MortonSrc src{p.mkeys, p.mvals, morton_decoder(p)};
+        return by_modes(p.N, [&](auto NC) { return model_values_n<decltype(NC)::value>(p, src, out); });
+    }
+    const SoaSrc src{slab_in(live_slab(p), p.N)};
+    return by_modes(p.N, [&](auto NC) { return model_values_n<decltype(NC)::value>(p, src, out); });
 }
 
 }  // namespace dgpu
@@ -202,7 +240,7 @@ int dgpu_mttkrp_all_modes(dgpu_plan* plan) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     if (!p) { set_error("dgpu_mttkrp_all_modes: null plan"); return DGPU_ERR_ARG; }
     DGPU_CUDA(cudaSetDevice(p->device));
-    return launch_mttkrp_all_modes(*p, live_slab(*p));
+    return launch_mttkrp_all_modes(*p);
 }
 
 int dgpu_model_values(dgpu_plan* plan, float* model_host) {
@@ -211,7 +249,7 @@ int dgpu_model_values(dgpu_plan* plan, float* model_host) {
     DGPU_CUDA(cudaSetDevice(p->device));
     float* d = nullptr;
     DGPU_TRY(dev_alloc(*p, (void**)&d, p->nnz * sizeof(float)));
-    int rc = launch_model_values(*p, live_slab(*p), d);
+    int rc = launch_model_values(*p, d);
     if (rc == DGPU_OK) {
         if (cudaMemcpyAsync(model_host, d, p->nnz * sizeof(float), cudaMemcpyDeviceToHost,
                             p->stream) != cudaSuccess ||
@@ -238,7 +276,7 @@ int dgpu_tensor_norm_sq(dgpu_plan* plan, double* norm_sq) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     if (!p || !norm_sq) { set_error("dgpu_tensor_norm_sq: null argument"); return DGPU_ERR_ARG; }
     DGPU_CUDA(cudaSetDevice(p->device));
-    return cp_tensor_norm(*p, live_slab(*p).vals, norm_sq);
+    return cp_tensor_norm(*p, live_vals(*p), norm_sq);
 }
 
 }  // extern "C"

@@ -181,6 +181,8 @@ Plan::~Plan() {
     dev_free(lambda);
     dev_free(la_work);
     dev_free(la_f32);
+    dev_free(mkeys);
+    dev_free(mvals);
     if (cp_loop_exec) cudaGraphExecDestroy(cp_loop_exec);
     dev_free(cp_st);
     if (cp_fit_host) cudaFreeHost(cp_fit_host);
@@ -524,6 +526,17 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     build_schedule(p);
     DGPU_TRY(plan_tables(p));
 
+    if (p.layout == DGPU_LAYOUT_MORTON) {
+        // keys + values replace the slabs (the shard tables above stay for
+        // plan queries only)
+        DGPU_TRY(morton_build(p, in_slab));
+        p.cur = 0;
+        p.next_mode = 0;
+        DGPU_TRY(plan_factors(p));
+        DGPU_TRY(sync_checked(p));
+        return DGPU_OK;
+    }
+
     // stable scatter of the input order into mode-0 shard order
     int res = 0;
     DGPU_TRY(stable_sort_pingpong(p, in_slab, 0, p.ident, 0, p.shift[0], p.K[0], &res));
@@ -611,7 +624,62 @@ static int check_order(Plan& p, int n, const Slab& s, int rows_sorted) {
     return DGPU_OK;
 }
 
+// A Morton file: keys and values are uploaded as they are and checked on
+// the device (decode within range, re-encode to the same key, ascending);
+// the decoded nonzeros give the shard tables for plan queries, then the
+// slabs are released.
+static int plan_build_dnp_morton(Plan& p, const DnpImage& img, const dgpu_plan_opts& o) {
+    dgpu_plan_opts oo = o;
+    oo.threads = img.threads;
+    oo.layout = DGPU_LAYOUT_MORTON;
+    DGPU_TRY(plan_init(p, img.N, img.nnz, img.dims, oo));
+    uint64_t seen = 0;
+    for (int n = 0; n < p.N; ++n) {
+        const int pc = __builtin_popcountll(img.mmask[n]);
+        if (pc == 0 || pc > 32 || pc != img.mbits[n] || (img.mmask[n] & seen)) {
+            set_error("dnp: Morton mask of mode %d (%d bits, %u stated) is empty, too wide or "
+                      "overlaps another mode's", n, pc, (unsigned)img.mbits[n]);
+            return DGPU_ERR_IO;
+        }
+        seen |= img.mmask[n];
+        p.mmask[n] = img.mmask[n];
+        p.mbits[n] = img.mbits[n];
+        plan_mode_geometry(p, n, rows_per_shard(p.dims[n], p.T));
+    }
+    DGPU_TRY(plan_alloc_slabs(p));
+    DGPU_TRY(dev_alloc(p, (void**)&p.mkeys, p.nnz * sizeof(uint64_t)));
+    DGPU_TRY(dev_alloc(p, (void**)&p.mvals, p.nnz * sizeof(float)));
+    DGPU_CUDA(cudaMemcpyAsync(p.mkeys, img.mkeys.data(), p.nnz * sizeof(uint64_t),
+                              cudaMemcpyHostToDevice, p.stream));
+    DGPU_CUDA(cudaMemcpyAsync(p.mvals, img.mvals.data(), p.nnz * sizeof(float),
+                              cudaMemcpyHostToDevice, p.stream));
+    DGPU_TRY(morton_check_decode(p, 1));
+    DGPU_TRY(device_shard_counts(p, p.slab[1], p.count));
+    p.sbeg.assign(p.N, {});
+    p.send.assign(p.N, {});
+    for (int n = 0; n < p.N; ++n) {
+        p.sbeg[n].resize(p.K[n]);
+        p.send[n].resize(p.K[n]);
+        uint64_t c = 0;
+        for (uint32_t s = 0; s < p.K[n]; ++s) {
+            p.sbeg[n][s] = c;
+            c += p.count[n][s];
+            p.send[n][s] = c;
+        }
+    }
+    build_schedule(p);
+    DGPU_TRY(plan_tables(p));
+    DGPU_TRY(sync_checked(p));
+    free_slabs(p);
+    p.cur = 0;
+    p.next_mode = 0;
+    DGPU_TRY(plan_factors(p));
+    DGPU_TRY(sync_checked(p));
+    return DGPU_OK;
+}
+
 int plan_build_dnp(Plan& p, const DnpImage& img, const dgpu_plan_opts& o) {
+    if (img.layout == DGPU_LAYOUT_MORTON) return plan_build_dnp_morton(p, img, o);
     dgpu_plan_opts oo = o;
     oo.threads = img.threads;
     oo.layout = img.layout;

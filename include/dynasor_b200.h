@@ -49,10 +49,17 @@ extern "C" {
 /* ---- layouts / kernels (values match the reference enums) ------------ */
 #define DGPU_LAYOUT_PINGPONG 0   /* Layout::PingPong: remap every mode    */
 #define DGPU_LAYOUT_NCOPY    1   /* Layout::NCopy: N pre-sorted copies    */
+/* Layout::Morton (include/dynasor_common.h:133-155, src/dynasor_morton.cpp):
+ * one 64-bit key per nonzero interleaving the mode indices (LSB-first round
+ * robin, sum of ceil(log2 I_n) <= 64) plus the value, sorted by key; 12 bytes
+ * per nonzero.  Only the all-modes pass runs on it (dgpu_mttkrp_all_modes,
+ * dgpu_mttkrp_sweep, CP-ALS as Jacobi); dgpu_mttkrp_mode gives
+ * DGPU_ERR_ARG.  dgpu_plan_morton reads the masks, keys and values. */
+#define DGPU_LAYOUT_MORTON   4
 /* Layout chosen from the device-memory budget like dyn_plan_storage
  * (src/dynasor_preprocess.cpp:951-1104): NCopy when it fits, else PingPong.
- * dgpu_plan_info.layout reports the choice. */
-#define DGPU_LAYOUT_AUTO     2
+ * dgpu_plan_info.layout reports the choice.  (Not a reference enum value.) */
+#define DGPU_LAYOUT_AUTO     16
 
 #define DGPU_CP_GAUSS_SEIDEL 0   /* CpKernel::GaussSeidel                 */
 #define DGPU_CP_JACOBI       1   /* CpKernel::Jacobi (all-modes pass)     */
@@ -255,10 +262,18 @@ int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y,
                            float* const* Yhat, double* secs);
 
 /* Current slab as the next mode's kernel will read it (bit-exact layout
- * checks against the reference's Tensor after process(n)). */
+ * checks against the reference's Tensor after process(n)).  A Morton plan
+ * gives its nonzeros in key order with the indices decoded from the keys. */
 int dgpu_download_slab(dgpu_plan* plan, float* vals, uint32_t* const* idx);
 /* NCopy copy k (layout NCopy only). */
 int dgpu_download_copy(dgpu_plan* plan, int k, float* vals, uint32_t* const* idx);
+/* Morton layout state (T.morton_mask / morton_bits / morton_keys /
+ * morton_vals after build_morton_layout, src/dynasor_morton.cpp:143-352):
+ * mask[n] and bits[n] for n < num_modes, and, when keys / vals are not
+ * NULL, the nnz sorted keys and their values.  DGPU_ERR_NOT_BUILT unless
+ * the plan's layout is DGPU_LAYOUT_MORTON.  Synchronises the plan stream. */
+int dgpu_plan_morton(dgpu_plan* plan, uint64_t* mask, uint8_t* bits, uint64_t* keys,
+                     float* vals);
 
 /* ---- CP-ALS (replaces cpals, src/dynasor_cpals.cpp:120-396) ---------- */
 void dgpu_cp_options_default(dgpu_cp_options* opt);

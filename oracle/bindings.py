@@ -84,6 +84,9 @@ def _oracle_lib():
         L.orc_remap.argtypes = [C.c_void_p, C.c_int]
         L.orc_process_layout.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.orc_ncopy.argtypes = [C.c_void_p, C.c_int, C.c_int, _f32p, C.c_void_p]
+        L.orc_morton.restype = C.c_int
+        L.orc_morton.argtypes = [C.c_int, C.c_uint64, _u32p, _f32p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_mttkrp_f32_fold.argtypes = [C.c_int, C.c_uint64, _f32p, C.c_void_p, C.c_int,
                                           C.c_int, C.c_void_p, _f32p, C.c_uint32]
         L.orc_mttkrp_f64.argtypes = [C.c_int, C.c_uint64, _f32p, C.c_void_p, C.c_int, C.c_int,
@@ -178,6 +181,22 @@ def mttkrp_f32_fold(vals, idx, n, Y, dim_n):
     L.orc_mttkrp_f32_fold(N, len(vals), np.ascontiguousarray(vals, np.float32), _ptr_array(idx),
                           n, Rp, _ptr_array(Y), out, dim_n)
     return out
+
+
+def morton(dims, vals, idx):
+    """The oracle's Morton layout: (mask, bits, sorted keys, values), or None
+    when the mode sizes need more than 64 key bits."""
+    N = len(dims)
+    mask = np.zeros(N, np.uint64)
+    bits = np.zeros(N, np.uint8)
+    keys = np.zeros(len(vals), np.uint64)
+    vo = np.zeros(len(vals), np.float32)
+    idx = [np.ascontiguousarray(i, np.uint32) for i in idx]
+    rc = _oracle_lib().orc_morton(N, len(vals), np.ascontiguousarray(dims, np.uint32),
+                                  np.ascontiguousarray(vals, np.float32), _ptr_array(idx),
+                                  mask.ctypes.data, bits.ctypes.data, keys.ctypes.data,
+                                  vo.ctypes.data)
+    return None if rc != 0 else (mask, bits, keys, vo)
 
 
 def mttkrp_f64(vals, idx, n, Y, R, dim_n):
@@ -286,6 +305,12 @@ def _ref_lib():
         L.ref_save_dnp.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_load_dnp.restype = C.c_void_p
         L.ref_load_dnp.argtypes = [C.c_char_p, C.c_int, C.c_int]
+        L.ref_build_morton.restype = C.c_int
+        L.ref_build_morton.argtypes = [C.c_void_p]
+        L.ref_morton_get.restype = C.c_int
+        L.ref_morton_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_all_modes_morton.restype = C.c_double
+        L.ref_all_modes_morton.argtypes = [C.c_void_p]
         _rlib = L
     return _rlib
 
@@ -329,6 +354,24 @@ class Reference:
         self.N, self.dims, self.nnz, self.Rp = N, dims, int(nnz), None
         self._plan_facts(threads)
         return self
+
+    def build_morton(self):
+        """build_morton_layout on the built tensor (src/dynasor_morton.cpp:143-352)."""
+        assert self.L.ref_build_morton(self.h) == 0
+
+    def morton(self):
+        """(mask[N] u64, bits[N] u8, sorted keys u64, values f32)."""
+        mask = np.zeros(self.N, np.uint64)
+        bits = np.zeros(self.N, np.uint8)
+        keys = np.zeros(self.nnz, np.uint64)
+        vals = np.zeros(self.nnz, np.float32)
+        rc = self.L.ref_morton_get(self.h, mask.ctypes.data, bits.ctypes.data, keys.ctypes.data,
+                                   vals.ctypes.data)
+        assert rc == 0
+        return mask, bits, keys, vals
+
+    def all_modes_morton(self):
+        return self.L.ref_all_modes_morton(self.h)
 
     def save_dnp(self, path):
         """save_dnp_tensor on the built tensor (src/dynasor_dnp.cpp:639-700)."""

@@ -22,6 +22,8 @@
 //      both as the reference's own FP32 fold (fmaf, slab order) and in FP64
 //    * CP-ALS (Gauss-Seidel) in FP64  [src/dynasor_cpals.cpp:42-396,
 //                                      src/dynasor_linalg.cpp:47-402]
+//    * the Morton bit plan, keys and key order
+//                                     [src/dynasor_morton.cpp:43-134, 143-352]
 //
 //  The LPT sort uses std::sort with the same strict-weak ordering as the
 //  reference, so shard order on count ties follows the same libstdc++
@@ -542,6 +544,46 @@ void orc_ncopy(void* h, int k, int fiber_on, float* vals, uint32_t* const* idx) 
     if (fiber_on && o->kclass[k] == 2) orc_fiber_sort(h, k);
     orc_get_slab(h, vals, idx);
     o->cur = std::move(saved);
+}
+
+// Morton layout: per-mode bit counts b_n = ceil(log2 I_n) (at least 1),
+// bit positions handed out LSB-first round-robin over the modes that still
+// need bits; key = OR over modes of the index bits placed at the mode's
+// positions; (key, value) pairs stably sorted by key.  -1 when sum b_n > 64.
+int orc_morton(int N, uint64_t nnz, const uint32_t* dims, const float* vals,
+               const uint32_t* const* idx, uint64_t* mask, uint8_t* bits,
+               uint64_t* keys_out, float* vals_out)
+{
+    int need[8] = {0};
+    int total = 0;
+    for (int n = 0; n < N; ++n) {
+        int b = 1;
+        if (dims[n] > 1) { b = 0; for (uint32_t m = dims[n] - 1; m; m >>= 1) ++b; }
+        need[n] = b;
+        bits[n] = (uint8_t)b;
+        total += b;
+        mask[n] = 0;
+    }
+    if (total > 64) return -1;
+    std::vector<std::vector<int>> pos(N);
+    int at = 0;
+    while (at < total)
+        for (int n = 0; n < N && at < total; ++n)
+            if ((int)pos[n].size() < need[n]) { pos[n].push_back(at); mask[n] |= 1ull << at; ++at; }
+    std::vector<std::pair<uint64_t, float>> kv(nnz);
+    for (uint64_t i = 0; i < nnz; ++i) {
+        uint64_t k = 0;
+        for (int n = 0; n < N; ++n)
+            for (int j = 0; j < need[n]; ++j)
+                if ((idx[n][i] >> j) & 1u) k |= 1ull << pos[n][j];
+        kv[i] = {k, vals[i]};
+    }
+    std::stable_sort(kv.begin(), kv.end(),
+                     [](const std::pair<uint64_t, float>& a, const std::pair<uint64_t, float>& b) {
+                         return a.first < b.first;
+                     });
+    for (uint64_t i = 0; i < nnz; ++i) { keys_out[i] = kv[i].first; vals_out[i] = kv[i].second; }
+    return 0;
 }
 
 } // extern "C"

@@ -11,6 +11,8 @@
 //    * spmttkrp_reference      (src/dynasor_reference.cpp:18-50)
 //    * cpals                   (src/dynasor_cpals.cpp:120-396)
 //    * save_dnp_tensor / load_dnp_tensor (src/dynasor_dnp.cpp:639-803)
+//    * build_morton_layout / spmttkrp_all_modes_morton
+//                              (src/dynasor_morton.cpp:143-352, 612-784)
 //
 //  and to read back the FLYCOO plan tables and the SoA slab after each
 //  process(n), which is what the bit-exact remap parity tests compare.
@@ -20,6 +22,7 @@
 #include "dynasor_common.h"
 #include "dynasor_cpals.h"
 #include "dynasor_dnp.h"
+#include "dynasor_morton.h"
 #include "dynasor_linalg.h"
 
 #include <cstdint>
@@ -287,6 +290,36 @@ int ref_simd_width_hint(void) {
 #else
     return 4;
 #endif
+}
+
+// build_morton_layout on a built (PingPong / InPlace) tensor; 0 on success.
+int ref_build_morton(void* hp)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    Quiet q(h->quiet);
+    return build_morton_layout(h->T, h->threads) ? 0 : -1;
+}
+
+// Morton masks / bits and (when not null) the sorted keys and values.
+int ref_morton_get(void* hp, uint64_t* mask, uint8_t* bits, uint64_t* keys, float* vals)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    if (h->T.layout != Layout::Morton || !h->T.morton_keys) return -1;
+    for (int n = 0; n < h->T.num_modes; ++n) {
+        mask[n] = h->T.morton_mask[n];
+        bits[n] = h->T.morton_bits[n];
+    }
+    if (keys) std::memcpy(keys, h->T.morton_keys, h->T.nnz * sizeof(uint64_t));
+    if (vals) std::memcpy(vals, h->T.morton_vals, h->T.nnz * sizeof(float));
+    return 0;
+}
+
+// spmttkrp_all_modes_morton into F.Yhat; returns its seconds.
+double ref_all_modes_morton(void* hp)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    Quiet q(h->quiet);
+    return spmttkrp_all_modes_morton(h->T, h->F, h->threads);
 }
 
 // The reference's .dnp writer on the built tensor; 0 on success.
