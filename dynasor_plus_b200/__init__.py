@@ -118,7 +118,7 @@ class Plan:
         """A plan from a .dnp processed-tensor file (the reference's
         runtime-only mode, load_dnp_tensor): its slab(s), shard tables and
         schedule are used as they are.  `threads` must equal the file's
-        thread count; the file decides the layout (PingPong or NCopy).
+        thread count; the file decides the layout (PingPong, NCopy or Morton).
         `fiber` applies to PingPong files (NCopy copies record it)."""
         L = lib()
         info = dnp_peek(path)

@@ -190,14 +190,15 @@ int  dgpu_dnp_peek(const char* path, dgpu_dnp_info* info);
  * reference rejects a mismatch); the file decides layout, rows per shard and
  * kernel classes (opts->layout and ->mn_target are ignored; so is
  * opts->fiber for NCopy files, whose copies say whether they are
- * fiber-sorted).  PingPong and NCopy files only: Morton and InPlace files
- * give DGPU_ERR_ARG. */
+ * fiber-sorted).  Morton files give a Morton plan: keys and values are
+ * uploaded as they are and checked on the device (indices in range, keys
+ * canonical and ascending).  InPlace files give DGPU_ERR_ARG. */
 int  dgpu_plan_create_from_dnp(const char* path, const dgpu_plan_opts* opts,
                                dgpu_plan** plan);
 
 /* Write the plan as a .dnp file (replaces save_dnp_tensor,
  * include/dynasor_dnp.h:121-123).  PingPong plans between sweeps (next mode
- * 0; DGPU_ERR_ORDER otherwise), NCopy plans at any time.  A plan built from
+ * 0; DGPU_ERR_ORDER otherwise), NCopy and Morton plans at any time.  A plan built from
  * the same tensor with the same threads and layout writes the bytes the
  * reference writes after build_flycoo (NCopy: fiber-sorted copies carry
  * their CSR row pointers, as with --ncopy-csr-compact off).  Synchronises
