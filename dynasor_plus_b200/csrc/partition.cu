@@ -297,12 +297,13 @@ __device__ __forceinline__ void wc_unswizzle(uint32_t (&u)[8], uint32_t b) {
 }
 
 // Window size of the scatter and its buffer column count: N+1 input
-// columns; staging needs a 16-byte record + destination (5 words) when
-// N <= 3, else N+2 columns.
+// columns; staging needs a 16-byte record (4 words) when N <= 3, else the
+// N+1 columns again.  A staged element's destination is recomputed at
+// write-out from its key, so it is not stored.
 template <int N>
 constexpr int scatter_window() { return N <= 4 ? DGPU_SCAT_WINDOW : DGPU_SCAT_WINDOW / 2; }
 template <int N>
-constexpr int scatter_cols() { return N + 1 <= 4 ? 5 : N + 2; }
+constexpr int scatter_cols() { return N + 1 <= 4 ? 4 : N + 1; }
 
 // Persistent CTAs of 512 threads take chunks from a work queue (largest
 // first).  A chunk is walked in windows of W elements; while window k is
@@ -331,7 +332,6 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     // staged element: one 16-byte record (val, idx...) when N <= 3, else columns
     constexpr bool kRec = (N + 1 <= 4);
     constexpr int C = scatter_cols<N>();          // buffer columns (input, then stage)
-    constexpr int DC = kRec ? 4 : N + 1;          // column holding staged destinations
     constexpr int BPT = (kMaxBuckets + kScatThreads - 1) / kScatThreads;  // buckets per thread, at most
     extern __shared__ __align__(128) uint32_t sm[];
     __shared__ __align__(8) uint64_t bar[2];
@@ -488,7 +488,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                 }
             }
             __syncthreads();       // (3)
-            // c. stage in bucket order with each element's destination
+            // c. stage in bucket order
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
@@ -505,24 +505,30 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 #pragma unroll
                     for (int m = 0; m < N; ++m) bk[(size_t)(m + 1) * BW + lp] = id[s][m];
                 }
-                bk[(size_t)DC * BW + lp] = bd.y + lp;
             }
             __syncwarp();
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 if (key[s] != 0xffffffffu) wc[wc_slot(key[s], warp)] = 0;
             __syncthreads();       // (4)
-            // d. write-out: runs of one bucket are contiguous
+            // d. write-out: runs of one bucket are contiguous; slot i of
+            //    bucket b goes to (cursor of b before this window) + i - (the
+            //    bucket's first slot), i.e. ld[b].y + i, b from the element's key
             for (uint32_t i = threadIdx.x; i < cnt; i += kScatThreads) {
-                const uint32_t d = bk[(size_t)DC * BW + i];
-                if (d >= total) { atomicOr(err, kErrPartRange); continue; }
                 if constexpr (kRec) {
                     const uint4 r = reinterpret_cast<const uint4*>(bk)[i];
                     const uint32_t rv[4] = {r.x, r.y, r.z, r.w};
+                    const uint32_t kv = key_mode == 0 ? r.y : (key_mode == 1 ? r.z : r.w);
+                    const uint32_t kb = part_key(kv, shift, mask);
+                    const uint32_t d = kb < nb ? ld[kb].y + i : total;
+                    if (d >= total) { atomicOr(err, kErrPartRange); continue; }
                     out.vals[d] = __uint_as_float(rv[0]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = rv[m + 1];
                 } else {
+                    const uint32_t kb = part_key(bk[(size_t)(key_mode + 1) * BW + i], shift, mask);
+                    const uint32_t d = kb < nb ? ld[kb].y + i : total;
+                    if (d >= total) { atomicOr(err, kErrPartRange); continue; }
                     out.vals[d] = __uint_as_float(bk[i]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = bk[(size_t)(m + 1) * BW + i];
