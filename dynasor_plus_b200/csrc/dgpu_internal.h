@@ -75,7 +75,7 @@ struct Chunk {
     uint32_t tile_begin;
     uint32_t tile_end;
     uint32_t seg;
-    uint32_t pad;
+    uint32_t contiguous;        // 1: the tiles are consecutive slab ranges
 };
 
 // A segment: chunks [chunk_begin, chunk_end) sorted as one independent

@@ -66,10 +66,45 @@ __device__ __forceinline__ uint32_t part_key(uint32_t v, int shift, uint32_t mas
     return (v >> shift) & mask;
 }
 
+// Counts the keys of positions [begin, begin + count) into hc: scalar head
+// up to a 16-byte boundary (the column starts 256-byte aligned), 16-byte
+// loads four at a time (16 keys per thread in flight), scalar tail.
+__device__ __forceinline__ void hist_range(const uint32_t* __restrict__ keycol, uint32_t begin,
+                                           uint32_t count, int shift, uint32_t mask,
+                                           uint32_t* hc)
+{
+    const uint32_t* k = keycol + begin;
+    const uint32_t head = min(count, (4u - (begin & 3u)) & 3u);
+    for (uint32_t j = threadIdx.x; j < head; j += blockDim.x)
+        atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
+    const uint32_t n4 = (count - head) >> 2;
+    const uint4* k4 = reinterpret_cast<const uint4*>(k + head);
+    for (uint32_t i = threadIdx.x; i < n4; i += 4 * blockDim.x) {
+        uint4 a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t ii = i + u * blockDim.x;
+            a[u] = ii < n4 ? __ldg(k4 + ii) : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i + u * blockDim.x >= n4) break;
+            atomicAdd(&hc[part_key(a[u].x, shift, mask)], 1u);
+            atomicAdd(&hc[part_key(a[u].y, shift, mask)], 1u);
+            atomicAdd(&hc[part_key(a[u].z, shift, mask)], 1u);
+            atomicAdd(&hc[part_key(a[u].w, shift, mask)], 1u);
+        }
+    }
+    for (uint32_t j = head + 4 * n4 + threadIdx.x; j < count; j += blockDim.x)
+        atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
+}
+
 // One CTA per chunk.  With `copies` > 1 every warp group counts into its
 // own copy of the histogram (fewer shared-atomic collisions on skewed keys:
 // hot rows of a Zipf mode land in few buckets); the copies are summed at the
-// end.
+// end.  A chunk whose tiles are consecutive slab ranges (Chunk::contiguous = 1:
+// identity order and the shard-segmented fiber sorts) is counted as one
+// range, so no tile descriptor load sits between its key loads.
 __global__ void __launch_bounds__(kHistThreads)
 k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles,
              const Chunk* __restrict__ chunks, int shift, uint32_t mask, uint32_t nb,
@@ -80,34 +115,14 @@ k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles
     __syncthreads();
     uint32_t* hc = h + (size_t)((threadIdx.x >> 5) % copies) * nb;
     const Chunk c = chunks[blockIdx.x];
-    for (uint32_t t = c.tile_begin; t < c.tile_end; ++t) {
-        const Tile tl = tiles[t];
-        const uint32_t* k = keycol + tl.begin;
-        // scalar head up to a 16-byte boundary (the column starts 256-byte
-        // aligned), 16-byte loads two at a time (8 keys per thread in
-        // flight), scalar tail
-        const uint32_t head = min(tl.count, (4u - (tl.begin & 3u)) & 3u);
-        for (uint32_t j = threadIdx.x; j < head; j += blockDim.x)
-            atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
-        const uint32_t n4 = (tl.count - head) >> 2;
-        const uint4* k4 = reinterpret_cast<const uint4*>(k + head);
-        for (uint32_t i = threadIdx.x; i < n4; i += 2 * blockDim.x) {
-            const uint4 a = __ldg(k4 + i);
-            const bool two = i + blockDim.x < n4;
-            const uint4 b = two ? __ldg(k4 + i + blockDim.x) : make_uint4(0u, 0u, 0u, 0u);
-            atomicAdd(&hc[part_key(a.x, shift, mask)], 1u);
-            atomicAdd(&hc[part_key(a.y, shift, mask)], 1u);
-            atomicAdd(&hc[part_key(a.z, shift, mask)], 1u);
-            atomicAdd(&hc[part_key(a.w, shift, mask)], 1u);
-            if (two) {
-                atomicAdd(&hc[part_key(b.x, shift, mask)], 1u);
-                atomicAdd(&hc[part_key(b.y, shift, mask)], 1u);
-                atomicAdd(&hc[part_key(b.z, shift, mask)], 1u);
-                atomicAdd(&hc[part_key(b.w, shift, mask)], 1u);
-            }
+    if (c.contiguous && c.tile_end > c.tile_begin) {
+        const Tile a = tiles[c.tile_begin], z = tiles[c.tile_end - 1];
+        hist_range(keycol, a.begin, z.begin + z.count - a.begin, shift, mask, hc);
+    } else {
+        for (uint32_t t = c.tile_begin; t < c.tile_end; ++t) {
+            const Tile tl = tiles[t];
+            hist_range(keycol, tl.begin, tl.count, shift, mask, hc);
         }
-        for (uint32_t j = head + 4 * n4 + threadIdx.x; j < tl.count; j += blockDim.x)
-            atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
     }
     __syncthreads();
     uint32_t* out = cnt + (size_t)blockIdx.x * nb;
@@ -342,8 +357,9 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     const uint32_t nbp = (nb + 7u) & ~7u;
     uint32_t* buf = sm;                                      // [2][C][BW]
     uint32_t* cursor = buf + 2 * C * BW;                     // [nbp]
-    uint2* ld = reinterpret_cast<uint2*>(cursor + nbp);      // [nbp] {window base, dest - slot}
-    uint16_t* wc = reinterpret_cast<uint16_t*>(ld + nbp);    // [nbp][16], see wc_slot
+    uint32_t* wbase = cursor + nbp;                          // [nbp] bucket's first window slot
+    uint32_t* wdst = wbase + nbp;                            // [nbp] destination - slot
+    uint16_t* wc = reinterpret_cast<uint16_t*>(wdst + nbp);  // [nbp][16], see wc_slot
     static_assert(kScatWarps == 16, "bucket counter rows hold 16 warps");
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -481,7 +497,8 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                     const uint32_t b = b0 + u;
                     if ((uint32_t)u < per && b < nb) {
                         const uint32_t cur = cursor[b];
-                        ld[b] = make_uint2(pre, cur - pre);
+                        wbase[b] = pre;
+                        wdst[b] = cur - pre;
                         cursor[b] = cur + tot[u];
                         pre += tot[u];
                     }
@@ -492,8 +509,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
-                const uint2 bd = ld[key[s]];
-                const uint32_t lp = bd.x + wc[wc_slot(key[s], warp)] + rk[s];
+                const uint32_t lp = wbase[key[s]] + wc[wc_slot(key[s], warp)] + rk[s];
                 if (lp >= cnt) { atomicOr(err, kErrPartRange); continue; }
                 if constexpr (kRec) {
                     uint32_t r[4] = {__float_as_uint(val[s]), 0u, 0u, 0u};
@@ -513,21 +529,21 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             __syncthreads();       // (4)
             // d. write-out: runs of one bucket are contiguous; slot i of
             //    bucket b goes to (cursor of b before this window) + i - (the
-            //    bucket's first slot), i.e. ld[b].y + i, b from the element's key
+            //    bucket's first slot), i.e. wdst[b] + i, b from the element's key
             for (uint32_t i = threadIdx.x; i < cnt; i += kScatThreads) {
                 if constexpr (kRec) {
                     const uint4 r = reinterpret_cast<const uint4*>(bk)[i];
                     const uint32_t rv[4] = {r.x, r.y, r.z, r.w};
                     const uint32_t kv = key_mode == 0 ? r.y : (key_mode == 1 ? r.z : r.w);
                     const uint32_t kb = part_key(kv, shift, mask);
-                    const uint32_t d = kb < nb ? ld[kb].y + i : total;
+                    const uint32_t d = kb < nb ? wdst[kb] + i : total;
                     if (d >= total) { atomicOr(err, kErrPartRange); continue; }
                     out.vals[d] = __uint_as_float(rv[0]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = rv[m + 1];
                 } else {
                     const uint32_t kb = part_key(bk[(size_t)(key_mode + 1) * BW + i], shift, mask);
-                    const uint32_t d = kb < nb ? ld[kb].y + i : total;
+                    const uint32_t d = kb < nb ? wdst[kb] + i : total;
                     if (d >= total) { atomicOr(err, kErrPartRange); continue; }
                     out.vals[d] = __uint_as_float(bk[i]);
 #pragma unroll
@@ -658,6 +674,13 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
             }
             sg[s].chunk_end = (uint32_t)ch.size();
         }
+    }
+    // chunks whose tiles are consecutive slab ranges
+    for (Chunk& c : ch) {
+        bool contiguous = true;
+        for (uint32_t t = c.tile_begin; t + 1 < c.tile_end && contiguous; ++t)
+            contiguous = tiles[t + 1].begin == tiles[t].begin + tiles[t].count;
+        c.contiguous = contiguous ? 1u : 0u;
     }
     // work order of the persistent scatter: largest chunks first
     std::vector<uint64_t> csize(ch.size(), 0);
