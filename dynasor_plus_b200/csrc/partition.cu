@@ -69,33 +69,34 @@ __device__ __forceinline__ uint32_t part_key(uint32_t v, int shift, uint32_t mas
 // Counts the keys of positions [begin, begin + count) into hc: scalar head
 // up to a 16-byte boundary (the column starts 256-byte aligned), 16-byte
 // loads four at a time (16 keys per thread in flight), scalar tail.
+// Threads `tid` of `nt` share the range.
 __device__ __forceinline__ void hist_range(const uint32_t* __restrict__ keycol, uint32_t begin,
                                            uint32_t count, int shift, uint32_t mask,
-                                           uint32_t* hc)
+                                           uint32_t* hc, uint32_t tid, uint32_t nt)
 {
     const uint32_t* k = keycol + begin;
     const uint32_t head = min(count, (4u - (begin & 3u)) & 3u);
-    for (uint32_t j = threadIdx.x; j < head; j += blockDim.x)
+    for (uint32_t j = tid; j < head; j += nt)
         atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
     const uint32_t n4 = (count - head) >> 2;
     const uint4* k4 = reinterpret_cast<const uint4*>(k + head);
-    for (uint32_t i = threadIdx.x; i < n4; i += 4 * blockDim.x) {
+    for (uint32_t i = tid; i < n4; i += 4 * nt) {
         uint4 a[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const uint32_t ii = i + u * blockDim.x;
+            const uint32_t ii = i + u * nt;
             a[u] = ii < n4 ? __ldg(k4 + ii) : make_uint4(0u, 0u, 0u, 0u);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            if (i + u * blockDim.x >= n4) break;
+            if (i + u * nt >= n4) break;
             atomicAdd(&hc[part_key(a[u].x, shift, mask)], 1u);
             atomicAdd(&hc[part_key(a[u].y, shift, mask)], 1u);
             atomicAdd(&hc[part_key(a[u].z, shift, mask)], 1u);
             atomicAdd(&hc[part_key(a[u].w, shift, mask)], 1u);
         }
     }
-    for (uint32_t j = head + 4 * n4 + threadIdx.x; j < count; j += blockDim.x)
+    for (uint32_t j = head + 4 * n4 + tid; j < count; j += nt)
         atomicAdd(&hc[part_key(__ldg(k + j), shift, mask)], 1u);
 }
 
@@ -104,7 +105,9 @@ __device__ __forceinline__ void hist_range(const uint32_t* __restrict__ keycol, 
 // hot rows of a Zipf mode land in few buckets); the copies are summed at the
 // end.  A chunk whose tiles are consecutive slab ranges (Chunk::contiguous = 1:
 // identity order and the shard-segmented fiber sorts) is counted as one
-// range, so no tile descriptor load sits between its key loads.
+// range, so no tile descriptor load sits between its key loads; otherwise
+// (processing order) each warp takes its own tiles, so the warps' loads
+// overlap.
 __global__ void __launch_bounds__(kHistThreads)
 k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles,
              const Chunk* __restrict__ chunks, int shift, uint32_t mask, uint32_t nb,
@@ -117,11 +120,13 @@ k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles
     const Chunk c = chunks[blockIdx.x];
     if (c.contiguous && c.tile_end > c.tile_begin) {
         const Tile a = tiles[c.tile_begin], z = tiles[c.tile_end - 1];
-        hist_range(keycol, a.begin, z.begin + z.count - a.begin, shift, mask, hc);
+        hist_range(keycol, a.begin, z.begin + z.count - a.begin, shift, mask, hc, threadIdx.x,
+                   blockDim.x);
     } else {
-        for (uint32_t t = c.tile_begin; t < c.tile_end; ++t) {
+        const uint32_t lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+        for (uint32_t t = c.tile_begin + (threadIdx.x >> 5); t < c.tile_end; t += nw) {
             const Tile tl = tiles[t];
-            hist_range(keycol, tl.begin, tl.count, shift, mask, hc);
+            hist_range(keycol, tl.begin, tl.count, shift, mask, hc, lane, 32u);
         }
     }
     __syncthreads();
