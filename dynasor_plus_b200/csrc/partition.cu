@@ -138,32 +138,45 @@ k_chunk_hist(const uint32_t* __restrict__ keycol, const Tile* __restrict__ tiles
     }
 }
 
-// grid (segments, ceil(nb/256)); thread = bucket.
-__global__ void __launch_bounds__(256)
+// grid (segments, ceil(nb/32)), 1024 threads: lane = bucket of the CTA's
+// 32, warp = one of 32 slices of the segment's chunks.  Each slice sums its
+// chunks, the slices' sums are prefixed in shared memory, then each slice
+// writes its chunks' exclusive offsets; the last slice's running total is
+// the segment total of the bucket.
+__global__ void __launch_bounds__(1024)
 k_col_scan(const uint32_t* __restrict__ cnt, const Seg* __restrict__ segs, uint32_t nb,
            uint32_t* __restrict__ off, uint32_t* __restrict__ segtot)
 {
-    const uint32_t b = blockIdx.y * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
+    __shared__ uint32_t part[32][33];
+    const uint32_t lane = threadIdx.x & 31u, sl = threadIdx.x >> 5;
+    const uint32_t b = blockIdx.y * 32u + lane;
     const Seg s = segs[blockIdx.x];
-    uint32_t run = 0;
-    uint32_t c = s.chunk_begin;
-    for (; c + 8 <= s.chunk_end; c += 8) {
-        uint32_t v[8];
+    const uint32_t nc = s.chunk_end - s.chunk_begin;
+    const uint32_t per = (nc + 31u) / 32u;
+    const uint32_t c0 = s.chunk_begin + min(nc, sl * per);
+    const uint32_t c1 = s.chunk_begin + min(nc, (sl + 1u) * per);
+    uint32_t sum = 0;
+    if (b < nb) {
+        uint32_t c = c0;
+        for (; c + 4 <= c1; c += 4) {
+            uint32_t v[4];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = cnt[(size_t)(c + k) * nb + b];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            off[(size_t)(c + k) * nb + b] = run;
-            run += v[k];
+            for (int k = 0; k < 4; ++k) v[k] = cnt[(size_t)(c + k) * nb + b];
+            sum += (v[0] + v[1]) + (v[2] + v[3]);
         }
+        for (; c < c1; ++c) sum += cnt[(size_t)c * nb + b];
     }
-    for (; c < s.chunk_end; ++c) {
+    part[sl][lane] = sum;
+    __syncthreads();
+    uint32_t run = 0;
+    for (uint32_t k = 0; k < sl; ++k) run += part[k][lane];
+    if (b >= nb) return;
+    for (uint32_t c = c0; c < c1; ++c) {
         const uint32_t v = cnt[(size_t)c * nb + b];
         off[(size_t)c * nb + b] = run;
         run += v;
     }
-    segtot[(size_t)blockIdx.x * nb + b] = run;
+    if (sl == 31u) segtot[(size_t)blockIdx.x * nb + b] = run;
 }
 
 // grid = segments, 1024 threads: base[s][b] = seg.base + sum_{b' < b} tot[s][b']
@@ -746,8 +759,8 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
     }
     {
         LaunchTimer t(p, p.part_fiber ? KK_FIB_SCAN : KK_PART_SCAN, (double)L.nchunks * nb * 8.0);
-        dim3 g(L.nsegs, (nb + 255) / 256);
-        k_col_scan<<<g, 256, 0, p.stream>>>(p.part_cnt, L.segs, nb, p.part_off, p.part_base);
+        dim3 g(L.nsegs, (nb + 31) / 32);
+        k_col_scan<<<g, 1024, 0, p.stream>>>(p.part_cnt, L.segs, nb, p.part_off, p.part_base);
         k_bucket_scan<<<L.nsegs, 1024, 0, p.stream>>>(p.part_base, L.segs, nb);
         DGPU_CUDA(cudaGetLastError());
     }
