@@ -57,6 +57,8 @@ constexpr int kHistThreads = 1024;
 #endif
 constexpr int kScatThreads = DGPU_SCAT_THREADS;   // threads of a scatter CTA
 constexpr int kScatWarps = kScatThreads / 32;
+// Most window buffers a scatter CTA uses (see scatter_bufs).
+constexpr int kScatBufsMax = 3;
 // Thread that issues a scatter CTA's bulk copies: the last one, whose warp
 // has no bucket-prefix work for up to kScatThreads / 2 buckets.
 constexpr int kIssuer = kScatThreads - 1;
@@ -337,6 +339,11 @@ template <int N>
 constexpr int scatter_window() { return N <= 4 ? DGPU_SCAT_WINDOW : DGPU_SCAT_WINDOW / 2; }
 template <int N>
 constexpr int scatter_cols() { return N + 1 <= 4 ? 4 : N + 1; }
+// Window buffers: three (window k+2 streams in while window k is ranked and
+// written) while two CTAs per SM still fit in shared memory (4-column
+// buffers, N <= 3), else two.
+template <int N>
+constexpr int scatter_bufs() { return scatter_cols<N>() <= 4 ? 3 : 2; }
 
 // Persistent CTAs of 512 threads take chunks from a work queue (largest
 // first).  A chunk is walked in windows of W elements; while window k is
@@ -367,14 +374,15 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
     constexpr int C = scatter_cols<N>();          // buffer columns (input, then stage)
     constexpr int BPT = (kMaxBuckets + kScatThreads - 1) / kScatThreads;  // buckets per thread, at most
     extern __shared__ __align__(128) uint32_t sm[];
-    __shared__ __align__(8) uint64_t bar[2];
+    constexpr int NBUF = scatter_bufs<N>();
+    __shared__ __align__(8) uint64_t bar[kScatBufsMax];
     __shared__ uint32_t wsum[kScatWarps];
     __shared__ uint32_t s_chunk[2];     // alternating: a slot is rewritten two barriers later
     __shared__ Tile s_tiles[kTileStage];
     __shared__ int fail;
     const uint32_t nbp = (nb + 7u) & ~7u;
-    uint32_t* buf = sm;                                      // [2][C][BW]
-    uint32_t* cursor = buf + 2 * C * BW;                     // [nbp]
+    uint32_t* buf = sm;                                      // [NBUF][C][BW]
+    uint32_t* cursor = buf + NBUF * C * BW;                  // [nbp]
     uint32_t* wbase = cursor + nbp;                          // [nbp] bucket's first window slot
     uint32_t* wdst = wbase + nbp;                            // [nbp] destination - slot
     uint16_t* wc = reinterpret_cast<uint16_t*>(wdst + nbp);  // [nbp][16], see wc_slot
@@ -386,12 +394,16 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
         reinterpret_cast<uint32_t*>(wc)[i] = 0;
     if (threadIdx.x == 0) {
         fail = 0;
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int k = 0; k < NBUF; ++k) mbar_init(&bar[k], 1);
         fence_mbar_init();
     }
-    uint32_t kw = 0;               // windows this CTA has started (mbarrier phases)
-    bool pending = false;          // a bulk copy into buf[kw & 1] is outstanding
+    // window k (counted over the CTA's life) streams into buffer k % NBUF
+    // and completes phase (k / NBUF) & 1 of that buffer's mbarrier
+    uint32_t kw = 0;               // window being processed
+    uint32_t issued = 0;           // windows whose bulk copies were issued
+    auto bufk = [&](uint32_t k) { return buf + (size_t)(k % NBUF) * C * BW; };
+    auto bark = [&](uint32_t k) { return &bar[k % NBUF]; };
+    auto park = [](uint32_t k) { return (k / NBUF) & 1u; };
 
     for (uint32_t it = 0;; ++it) {
         if (threadIdx.x == 0) s_chunk[it & 1] = atomicAdd(queue, 1u);
@@ -407,20 +419,33 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
         const uint32_t nst = min(kTileStage, c.tile_end - c.tile_begin);
         for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) s_tiles[i] = tiles[c.tile_begin + i];
         __syncthreads();           // tile descriptors staged
-        // first non-empty window of the chunk
+        // the chunk's first window (t, w0, tl), and with three buffers its
+        // second (t1, w1, tl1); with two buffers the second is found after
+        // barrier (1) of the first
         uint32_t t = c.tile_begin, w0 = 0u - (uint32_t)W;
         Tile tl = s_tiles[0];
         if (!next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, t, w0, tl)) continue;
         if (threadIdx.x == kIssuer)
-            issue_window<N, W>(buf + (size_t)(kw & 1) * C * BW, in, tl.begin + w0,
-                               min((uint32_t)W, tl.count - w0), &bar[kw & 1]);
-        pending = true;
+            issue_window<N, W>(bufk(kw), in, tl.begin + w0, min((uint32_t)W, tl.count - w0), bark(kw));
+        issued = kw + 1;
+        uint32_t t1 = t, w1 = w0;
+        Tile tl1 = tl;
+        bool has1 = false;
+        if constexpr (NBUF == 3) {
+            has1 = next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, t1, w1, tl1);
+            if (has1) {
+                if (threadIdx.x == kIssuer)
+                    issue_window<N, W>(bufk(kw + 1), in, tl1.begin + w1,
+                                       min((uint32_t)W, tl1.count - w1), bark(kw + 1));
+                issued = kw + 2;
+            }
+        }
 
         for (;;) {
             const uint32_t cnt = min((uint32_t)W, tl.count - w0);
             const uint32_t head = (tl.begin + w0) & 3u;
-            uint32_t* bk = buf + (size_t)(kw & 1) * C * BW;
-            if (!mbar_wait(&bar[kw & 1], (kw >> 1) & 1u)) {
+            uint32_t* bk = bufk(kw);
+            if (!mbar_wait(bark(kw), park(kw))) {
                 fail = 1;
                 atomicOr(err, kErrPartWait);
             }
@@ -456,15 +481,28 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             }
             __syncthreads();       // (1) buffer read, counters complete, `fail` visible
             if (fail) break;
-            pending = false;
-            // prefetch the next window into the other buffer: its last reader
-            // (window kw-1's write-out) finished before barrier (1)
-            uint32_t nt = t, nw0 = w0;
-            Tile ntl = tl;
-            const bool more = next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, nt, nw0, ntl);
-            if (more && threadIdx.x == kIssuer)
-                issue_window<N, W>(buf + (size_t)((kw + 1) & 1) * C * BW, in, ntl.begin + nw0,
-                                   min((uint32_t)W, ntl.count - nw0), &bar[(kw + 1) & 1]);
+            // prefetch window kw + NBUF - 1 into the buffer window kw-1
+            // used: its write-out finished before barrier (1)
+            uint32_t t2 = t1, w2 = w1;
+            Tile tl2 = tl1;
+            bool has2 = false;
+            if constexpr (NBUF == 3) {
+                has2 = has1 && next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, t2, w2, tl2);
+                if (has2) {
+                    if (threadIdx.x == kIssuer)
+                        issue_window<N, W>(bufk(kw + 2), in, tl2.begin + w2,
+                                           min((uint32_t)W, tl2.count - w2), bark(kw + 2));
+                    issued = kw + 3;
+                }
+            } else {
+                has1 = next_window<W>(tiles, s_tiles, c.tile_begin, c.tile_end, t1, w1, tl1);
+                if (has1) {
+                    if (threadIdx.x == kIssuer)
+                        issue_window<N, W>(bufk(kw + 1), in, tl1.begin + w1,
+                                           min((uint32_t)W, tl1.count - w1), bark(kw + 1));
+                    issued = kw + 2;
+                }
+            }
             // b. warp prefixes per bucket (only counters a warp used become
             //    prefixes, so the warps' resets in c leave all counters zero)
             const uint32_t per = (nb + kScatThreads - 1) / kScatThreads;
@@ -570,14 +608,20 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             }
             fence_proxy_async_smem();   // generic accesses before a later bulk write
             ++kw;
-            if (!more) break;
-            pending = true;
-            t = nt; w0 = nw0; tl = ntl;
+            if (!has1) break;
+            t = t1; w0 = w1; tl = tl1;
+            if constexpr (NBUF == 3) {
+                t1 = t2; w1 = w2; tl1 = tl2; has1 = has2;
+            } else {
+                has1 = false;
+            }
         }
         if (fail) break;
     }
-    // leave no bulk copy in flight into this CTA's shared memory
-    if (fail && pending && threadIdx.x == kIssuer) mbar_wait(&bar[kw & 1], (kw >> 1) & 1u);
+    // leave no bulk copy in flight into this CTA's shared memory: on a
+    // failure, windows kw .. issued-1 may still be streaming
+    if (fail && threadIdx.x == kIssuer)
+        for (uint32_t k = kw; k < issued; ++k) mbar_wait(bark(k), park(k));
 }
 
 
@@ -585,7 +629,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 template <int N>
 size_t scatter_smem(uint32_t nb) {
     const size_t nbp = (nb + 7u) & ~7u;
-    return (2 * (size_t)scatter_cols<N>() * win_stride<scatter_window<N>()>() + 3 * nbp) * 4 +
+    return (scatter_bufs<N>() * (size_t)scatter_cols<N>() * win_stride<scatter_window<N>()>() + 3 * nbp) * 4 +
            (size_t)kScatWarps * nbp * 2;
 }
 
