@@ -23,17 +23,14 @@ def _zipf(dims=(3000, 500, 200), draws=30000, seed=31):
 
 
 def _distinct(dims, nnz, seed):
-    """nnz distinct uniform coordinates (any mode count)."""
+    """Up to nnz distinct uniform coordinates (any mode count), random order."""
     rng = np.random.default_rng(seed)
-    total = int(np.prod([int(d) for d in dims], dtype=np.float64))
-    lin = rng.choice(total, size=nnz, replace=False) if total < 1 << 40 else \
-        np.unique(rng.integers(0, total, size=nnz))
-    idx, rem = [], lin.astype(np.uint64)
-    for d in reversed(dims):
-        idx.append((rem % np.uint64(d)).astype(np.uint32))
-        rem = rem // np.uint64(d)
-    idx = idx[::-1]
-    vals = rng.standard_normal(len(lin)).astype(np.float32)
+    coords = np.stack([rng.integers(0, int(d), size=int(nnz * 1.3), dtype=np.int64)
+                       for d in dims], 1)
+    _, first = np.unique(coords, axis=0, return_index=True)
+    coords = coords[np.sort(first)[:nnz]]
+    idx = [np.ascontiguousarray(coords[:, n], dtype=np.uint32) for n in range(len(dims))]
+    vals = rng.standard_normal(len(coords)).astype(np.float32)
     return np.asarray(dims, np.uint32), vals, idx
 
 
@@ -42,6 +39,8 @@ CASES = [
     ("mode4", lambda: _distinct((50, 700, 9, 3000), 40000, 3)),
     ("tiny-modes", lambda: _distinct((1, 2, 3, 5, 1000), 2000, 4)),
     ("mode2-wide", lambda: _distinct((1 << 20, 70000), 50000, 5)),
+    # 22 + 21 + 21 = 64 key bits: the high word is fully used
+    ("bits64", lambda: _distinct((1 << 22, 1 << 21, (1 << 21) - 5), 30000, 6)),
 ]
 
 
@@ -82,6 +81,36 @@ def test_device_morton_build_matches_oracle(bindings, name, make):
     order = np.lexsort(tuple(reversed(idx)))
     got = np.lexsort(tuple(reversed(six)))
     assert all(np.array_equal(a[order], c[got]) for a, c in zip(idx, six))
+    p.close()
+
+
+@pytest.mark.gpu
+def test_device_morton_rejects_more_than_64_key_bits():
+    import dynasor_plus_b200 as d
+    dims = np.array([1 << 22, 1 << 22, 1 << 22], np.uint32)
+    idx = [np.array([0, 1, 2], np.uint32) for _ in range(3)]
+    with pytest.raises(d.DgpuError) as e:
+        d.Plan(dims, np.ones(3, np.float32), idx, threads=2, rank=16, layout="morton")
+    assert "64 key bits" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_morton_single_nonzero_and_two_modes():
+    import dynasor_plus_b200 as d
+    dims = np.array([7, 5], np.uint32)
+    idx = [np.array([6], np.uint32), np.array([4], np.uint32)]
+    vals = np.array([2.5], np.float32)
+    p = d.Plan(dims, vals, idx, threads=1, rank=16, layout="morton")
+    m, b, k, v = p.morton()
+    assert list(b) == [3, 3] and v[0] == np.float32(2.5)
+    Y = [np.zeros((int(n), 16), np.float32) for n in dims]
+    Y[0][6, :] = 2.0
+    Y[1][4, :] = 3.0
+    for n in range(2):
+        p.set_factor(n, Y[n])
+    p.all_modes()
+    assert np.allclose(p.yhat(0)[6], 2.5 * 3.0) and np.allclose(p.yhat(1)[4], 2.5 * 2.0)
+    assert np.count_nonzero(p.yhat(0)) == 16 and np.count_nonzero(p.yhat(1)) == 16
     p.close()
 
 
