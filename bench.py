@@ -53,9 +53,9 @@ METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 # kernels stream the slab once per launch, so their traffic grows with nnz;
 # the bench scales these figures to its own nnz for `roofline.traffic`.
 NCU_DRAM_BYTES_PER_NNZ = {
-    "part_scatter": 29.49,     # k_chunk_scatter, all launches averaged
-    "fiber_scatter": 29.49,
-    "mttkrp": 47.29,           # k_mttkrp_rowrun, 3 modes averaged
+    "part_scatter": 29.35,     # k_chunk_scatter, all launches averaged
+    "fiber_scatter": 29.35,
+    "mttkrp": 47.01,           # k_mttkrp_rowrun, 3 modes averaged
 }
 
 
