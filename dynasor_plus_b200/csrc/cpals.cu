@@ -1014,7 +1014,10 @@ struct CpSession {
         DGPU_CUDA(cudaMemcpy(hs.data(), st, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
         const int last = (int)hs[0];
         const double tot = res.mttkrp_time_s + res.linalg_time_s;
-        const double fm = tot > 0 ? res.mttkrp_time_s / tot : 0.5;
+        // split of the loop's device time: this run's eager iteration, else
+        // the last measured one on this plan
+        const double fm = tot > 0 ? res.mttkrp_time_s / tot : p.cp_mttkrp_frac;
+        if (tot > 0) p.cp_mttkrp_frac = fm;
         res.mttkrp_time_s += fm * ms * 1e-3;
         res.linalg_time_s += (1.0 - fm) * ms * 1e-3;
         for (int i = it; i < last; ++i) {
@@ -1140,8 +1143,22 @@ int run_loop_cached(CpSession& s) {
 int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fit_history) {
     CpSession s(p, o, res, fit_history);
     DGPU_TRY(s.setup());
-    if (!s.done) DGPU_TRY(s.step_host());
-    if (s.loop_eligible()) DGPU_TRY(run_loop_cached(s));
+    // A plan whose device-loop graph was captured for this run's key runs
+    // every iteration, the first included, in that loop: the eager first
+    // iteration's work (allocation, tuning, timing split) was done by the
+    // run that captured it.
+    bool replayed = false;
+    if (s.graphs && !o.verbose && !s.done && p.cp_loop_exec) {
+        DGPU_TRY(s.ensure_state());
+        uint64_t key[12];
+        s.loop_key(key);
+        if (std::memcmp(key, p.cp_loop_key, sizeof(key)) == 0) {
+            DGPU_TRY(run_loop_cached(s));
+            replayed = true;
+        }
+    }
+    if (!replayed && !s.done) DGPU_TRY(s.step_host());
+    if (!replayed && s.loop_eligible()) DGPU_TRY(run_loop_cached(s));
     while (!s.done) DGPU_TRY(s.step_host());
     s.finish();
     return DGPU_OK;

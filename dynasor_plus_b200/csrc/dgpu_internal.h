@@ -220,6 +220,7 @@ struct Plan {
     cudaGraphExec_t cp_loop_exec = nullptr;
     uint64_t     cp_loop_key[12] = {};
     double       cp_tnorm2 = -1.0;              // ||T||^2 once computed (< 0: not yet)
+    double       cp_mttkrp_frac = 0.5;          // MTTKRP share of an iteration, last measured
     // Morton layout: sorted keys and their values (the slabs are freed once
     // they are built), per-mode masks and bit counts
     uint64_t*    mkeys = nullptr;
