@@ -313,14 +313,38 @@ k_small_solve(const double* __restrict__ Gd, int N, int n, int R, double ridge,
     double* Wx = reinterpret_cast<double*>(smraw);
     Real* A = reinterpret_cast<Real*>(Wx + RR);
     Real* invd = A + R * LDA;
-    for (int e = threadIdx.x; e < RR; e += 32) {
-        double v = 1.0;
-        for (int m = 0; m < N; ++m)
-            if (m != n) v *= Gd[(size_t)m * RR + e];
-        A[(e / R) * LDA + e % R] = (Real)v;
+    // Hadamard of the other modes' Grams, eight entries per lane at a time
+    // with every mode's loads issued before the products
+    for (int e0 = threadIdx.x; e0 < RR; e0 += 32 * 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = 1.0;
+        for (int m = 0; m < N; ++m) {
+            if (m == n) continue;
+            double g[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int e = e0 + 32 * u;
+                g[u] = e < RR ? __ldg(Gd + (size_t)m * RR + e) : 1.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] *= g[u];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + 32 * u;
+            if (e < RR) A[(e / R) * LDA + e % R] = (Real)v[u];
+        }
     }
     __syncwarp();
-    warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
+    // R <= 16: factor and map in registers (a 32-wide register version does
+    // not stay unrolled); wider ranks use the shared-memory solve
+    if (R <= 16) {
+        warp_ridge<Real>(A, LDA, R, ridge);
+        warp_chol_solve_map_reg<Real, 16>(A, LDA, R, invd, Wx);
+    } else {
+        warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
+    }
     for (int e = threadIdx.x; e < RR; e += 32) Wout[e] = Wx[e];
 }
 
@@ -373,47 +397,68 @@ k_update_small(double* __restrict__ Gd, float* __restrict__ G32, int N, int n, i
     // map was built by k_small_solve while this mode's MTTKRP ran.
     if (!Wpre && tid < 32) warp_chol_solve_map<Real>(A, LDA, R, invd, Wx, ridge);
     __syncthreads();
-    // Y = Yhat W (padding columns zero)
-    for (uint32_t e = tid; e < total; e += nt) {
-        const uint32_t i = e / Rp;
-        const int c = (int)(e - i * Rp);
-        if (c >= R) { Ys[e] = 0.f; continue; }
-        const float* yh = Hs + (size_t)i * Rp;
-        Real a0 = 0, a1 = 0;
-        int k = 0;
-        for (; k + 2 <= R; k += 2) {
-            a0 += (Real)yh[k] * (Real)Wx[k * R + c];
-            a1 += (Real)yh[k + 1] * (Real)Wx[(k + 1) * R + c];
+    // Y = Yhat W (padding columns zero): a thread takes one row and four
+    // columns, so each Yhat entry is read once per four outputs; every
+    // output keeps its even-k / odd-k partial sums
+    {
+        const int groups = Rp >> 2;
+        for (uint32_t w = tid; w < rows * (uint32_t)groups; w += nt) {
+            const uint32_t i = w / groups;
+            const int c0 = (int)(w - i * groups) * 4;
+            const float* yh = Hs + (size_t)i * Rp;
+            Real a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
+            int k = 0;
+            for (; k + 2 <= R; k += 2) {
+                const Real h0 = (Real)yh[k], h1 = (Real)yh[k + 1];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (c0 + q >= R) continue;
+                    a0[q] += h0 * (Real)Wx[k * R + c0 + q];
+                    a1[q] += h1 * (Real)Wx[(k + 1) * R + c0 + q];
+                }
+            }
+            if (k < R) {
+                const Real h0 = (Real)yh[k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (c0 + q < R) a0[q] += h0 * (Real)Wx[k * R + c0 + q];
+            }
+            float* ys = Ys + (size_t)i * Rp + c0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ys[q] = (c0 + q < R) ? (float)(a0[q] + a1[q]) : 0.f;
         }
-        if (k < R) a0 += (Real)yh[k] * (Real)Wx[k * R + c];
-        Ys[e] = (float)(a0 + a1);
     }
     __syncthreads();
-    // Gram of Y in FP64: thread = (entry, row slice)
+    // Gram of Y in FP64 over the upper triangle (a <= b): thread = (pair,
+    // row slice); the lower triangle is mirrored below
     {
-        const int slices = max(1, nt / RR);
-        const int pe = tid % RR, sl = tid / RR;
-        if (sl < slices && tid < RR * slices) {
-            const int a = pe / R, b = pe % R;
+        const int P = R * (R + 1) / 2;
+        const int slices = max(1, nt / P);
+        for (int t = tid; t < P * slices; t += nt) {
+            const int pair = t % P, sl = t / P;
+            int a = 0, rem = pair;
+            while (rem >= R - a) { rem -= R - a; ++a; }
+            const int b = a + rem;
             double acc = 0.0;
             for (uint32_t i = sl; i < rows; i += slices)
                 acc += (double)Ys[(size_t)i * Rp + a] * (double)Ys[(size_t)i * Rp + b];
-            atomicAdd(&G[pe], acc);
-        }
-        for (int e = tid + nt; e < RR; e += nt) {      // RR > nt: remaining entries
-            const int a = e / R, b = e % R;
-            double acc = 0.0;
-            for (uint32_t i = 0; i < rows; ++i)
-                acc += (double)Ys[(size_t)i * Rp + a] * (double)Ys[(size_t)i * Rp + b];
-            G[e] = acc;
+            atomicAdd(&G[a * R + b], acc);
         }
     }
     __syncthreads();
+    // lambda from the diagonal; 1/lambda per column (FP32, for the scaling);
+    // the Gram's lower triangle from its upper one
+    float* invc = reinterpret_cast<float*>(invd);           // R (the solve is done)
     for (int r = tid; r < R; r += nt) {
         const double l = sqrt(max(G[r * R + r], 0.0));
         lam[r] = l;
         lam64[r] = l;
         lambda[r] = (float)l;
+        invc[r] = l > 1e-20 ? (float)(1.0 / l) : 0.f;
+    }
+    for (int e = tid; e < RR; e += nt) {
+        const int a = e / R, b = e % R;
+        if (a > b) G[e] = G[b * R + a];
     }
     __syncthreads();
     for (int e = tid; e < RR; e += nt) {
@@ -425,12 +470,20 @@ k_update_small(double* __restrict__ Gd, float* __restrict__ G32, int N, int n, i
     }
     for (uint32_t e = tid; e < total; e += nt) {
         const int c = (int)(e % Rp);
-        if (c >= R) { Y[e] = 0.f; continue; }
-        const double l = lam[c];
-        const float inv = l > 1e-20 ? (float)(1.0 / l) : 0.f;
-        const float y = Ys[e] * inv;
-        Y[e] = y;
-        if (last) atomicAdd(&dot[c], (double)y * (double)Hs[e]);
+        Y[e] = c < R ? Ys[e] * invc[c] : 0.f;
+    }
+    if (last) {
+        // <Y_c, Yhat_c> per column: thread = (column, row slice)
+        const int slices = max(1, nt / R);
+        for (int t = tid; t < R * slices; t += nt) {
+            const int c = t % R, sl = t / R;
+            double acc = 0.0;
+            for (uint32_t i = sl; i < rows; i += slices) {
+                const size_t e = (size_t)i * Rp + c;
+                acc += (double)(Ys[e] * invc[c]) * (double)Hs[e];
+            }
+            atomicAdd(&dot[c], acc);
+        }
     }
     __syncthreads();
     if (!last) return;
