@@ -138,16 +138,38 @@ k_apply_map(const float* __restrict__ Yhat, uint32_t rows, int R, int Rp,
     Real* Ws = reinterpret_cast<Real*>(smem_raw);            // R x R
     for (int e = threadIdx.x; e < R * R; e += blockDim.x) Ws[e] = W[e];
     __syncthreads();
-    const size_t total = (size_t)rows * Rp;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
-        const size_t i = e / Rp;
-        const int c = (int)(e - i * Rp);
-        if (c >= R) { Y[e] = 0.f; continue; }
-        const float* yh = Yhat + i * Rp;
-        Real s = 0;
-        for (int k = 0; k < R; ++k) s += (Real)__ldg(yh + k) * Ws[(size_t)k * R + c];
-        Y[e] = (float)s;
+    // a thread takes one row and four columns: each Yhat entry is loaded
+    // once per four outputs (16-byte loads), each output keeps its single
+    // k-ordered sum
+    const int groups = Rp >> 2;
+    const size_t items = (size_t)rows * groups;
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < items;
+         w += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = w / groups;
+        const int c0 = (int)(w - i * groups) * 4;
+        const float4* yh = reinterpret_cast<const float4*>(Yhat + i * Rp);
+        Real s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int k4 = 0; k4 < R; k4 += 4) {
+            const float4 h4 = __ldg(yh + (k4 >> 2));
+            const float hv[4] = {h4.x, h4.y, h4.z, h4.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k4 + u;
+                if (k >= R) break;
+                const Real h = (Real)hv[u];
+                const Real* wr = Ws + (size_t)k * R + c0;
+                if (c0 < R) s0 += h * wr[0];
+                if (c0 + 1 < R) s1 += h * wr[1];
+                if (c0 + 2 < R) s2 += h * wr[2];
+                if (c0 + 3 < R) s3 += h * wr[3];
+            }
+        }
+        float4 out;
+        out.x = c0 < R ? (float)s0 : 0.f;
+        out.y = c0 + 1 < R ? (float)s1 : 0.f;
+        out.z = c0 + 2 < R ? (float)s2 : 0.f;
+        out.w = c0 + 3 < R ? (float)s3 : 0.f;
+        reinterpret_cast<float4*>(Y + i * Rp)[c0 >> 2] = out;
     }
 }
 
@@ -234,19 +256,38 @@ __global__ void __launch_bounds__(kLaThreads)
 k_scale_cols(float* __restrict__ Y, const float* __restrict__ Yhat, uint32_t rows, int R, int Rp,
              const double* __restrict__ lam64, double* __restrict__ dot_partial)
 {
-    extern __shared__ double sdot[];   // [R]
-    if (Yhat) for (int r = threadIdx.x; r < R; r += blockDim.x) sdot[r] = 0.0;
+    extern __shared__ double sdot[];   // [R], then R floats: 1 / lambda per column
+    float* invs = reinterpret_cast<float*>(sdot + R);
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        sdot[r] = 0.0;
+        const double l = lam64[r];
+        invs[r] = l > 1e-20 ? (float)(1.0 / l) : 0.f;
+    }
     __syncthreads();
     const size_t total = (size_t)rows * Rp;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % Rp);
-        if (c >= R) continue;
-        const double l = lam64[c];
-        const float inv = l > 1e-20 ? (float)(1.0 / l) : 0.f;
-        const float y = Y[e] * inv;
-        Y[e] = y;
-        if (Yhat) atomicAdd(&sdot[c], (double)y * (double)Yhat[e]);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (Yhat && stride % Rp == 0) {
+        // every element this thread visits is in one column: one atomic
+        const int c = (int)(first % Rp);
+        double acc = 0.0;
+        if (c < R) {
+            const float inv = invs[c];
+            for (size_t e = first; e < total; e += stride) {
+                const float y = Y[e] * inv;
+                Y[e] = y;
+                acc += (double)y * (double)Yhat[e];
+            }
+            atomicAdd(&sdot[c], acc);
+        }
+    } else {
+        for (size_t e = first; e < total; e += stride) {
+            const int c = (int)(e % Rp);
+            if (c >= R) continue;
+            const float y = Y[e] * invs[c];
+            Y[e] = y;
+            if (Yhat) atomicAdd(&sdot[c], (double)y * (double)Yhat[e]);
+        }
     }
     __syncthreads();
     if (Yhat)
@@ -651,6 +692,20 @@ int launch_small_solve(Plan& p, const LaLayout& L, int n, int solve_fp64, double
     return DGPU_OK;
 }
 
+// The large-mode solve map (FP64 Wd and its FP32 copy W32) on stream st.
+int launch_large_solve(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
+                       cudaStream_t st) {
+    if (solve_fp64)
+        k_build_solve_map<double><<<1, 1024, 0, st>>>(L.Gd, p.N, n, p.R, ridge, L.A, L.Wd, L.W32);
+    else
+        k_build_solve_map<float><<<1, 1024, 0, st>>>(L.Gd, p.N, n, p.R, ridge,
+                                                      reinterpret_cast<float*>(L.A), L.Wd, L.W32);
+    DGPU_CUDA(cudaGetLastError());
+    return DGPU_OK;
+}
+
+// Wpre != nullptr: the mode's solve map was already built (on the side
+// stream, while its MTTKRP ran) into L.Wd / L.W32.
 int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge, bool last,
                 double tn2, bool* fit_done, const double* Wpre = nullptr) {
     const size_t RR = (size_t)p.R * p.R;
@@ -677,8 +732,8 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
         *fit_done = last;
         return DGPU_OK;
     }
+    if (!Wpre) DGPU_TRY(launch_large_solve(p, L, n, solve_fp64, ridge, p.stream));
     if (solve_fp64) {
-        k_build_solve_map<double><<<1, 1024, 0, p.stream>>>(L.Gd, p.N, n, p.R, ridge, L.A, L.Wd, L.W32);
         const size_t sm = RR * sizeof(double);
         if (sm > 48 * 1024)
             DGPU_CUDA(cudaFuncSetAttribute(k_apply_map<double>,
@@ -686,8 +741,6 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
         k_apply_map<double><<<grid_for((size_t)p.dims[n] * p.Rp), kLaThreads, sm, p.stream>>>(
             p.Yhat[n], p.dims[n], p.R, p.Rp, L.Wd, p.Y[n]);
     } else {
-        k_build_solve_map<float><<<1, 1024, 0, p.stream>>>(L.Gd, p.N, n, p.R, ridge,
-                                                           reinterpret_cast<float*>(L.A), L.Wd, L.W32);
         const size_t sm = RR * sizeof(float);
         if (sm > 48 * 1024)
             DGPU_CUDA(cudaFuncSetAttribute(k_apply_map<float>,
@@ -698,7 +751,7 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
     DGPU_CUDA(cudaGetLastError());
     DGPU_TRY(gram_into(p, L, n, 1));
     const unsigned g = grid_for((size_t)p.dims[n] * p.Rp, kGramChunks);
-    k_scale_cols<<<g, kLaThreads, (size_t)p.R * sizeof(double), p.stream>>>(
+    k_scale_cols<<<g, kLaThreads, (size_t)p.R * (sizeof(double) + sizeof(float)), p.stream>>>(
         p.Y[n], last ? p.Yhat[n] : nullptr, p.dims[n], p.R, p.Rp, L.lam64, L.dot);
     DGPU_CUDA(cudaGetLastError());
     p.yb_stale[n] = true;
@@ -879,15 +932,18 @@ struct CpSession {
             for (int n = 0; n < p.N; ++n)
                 DGPU_TRY(p.layout == DGPU_LAYOUT_NCOPY ? mode_ncopy(p, n) : mode_pingpong(p, n));
         for (int n = 0; n < p.N; ++n) {
-            // Gauss-Seidel on a small mode: its solve map depends only on the
-            // other modes' Grams, so it is built on the side stream while
-            // this mode's MTTKRP runs (fork after the previous update, join
+            // Gauss-Seidel: a mode's solve map depends only on the other
+            // modes' Grams, so it is built on the side stream while this
+            // mode's MTTKRP runs (fork after the previous update, join
             // before this one)
-            const bool ovl = !jacobi && small_mode(p, n);
+            const bool ovl = !jacobi;
             if (ovl) {
                 DGPU_CUDA(cudaEventRecord(fork[n], p.stream));
                 DGPU_CUDA(cudaStreamWaitEvent(p.side_stream, fork[n], 0));
-                DGPU_TRY(launch_small_solve(p, L, n, o.solve_fp64, o.ridge, p.side_stream));
+                if (small_mode(p, n))
+                    DGPU_TRY(launch_small_solve(p, L, n, o.solve_fp64, o.ridge, p.side_stream));
+                else
+                    DGPU_TRY(launch_large_solve(p, L, n, o.solve_fp64, o.ridge, p.side_stream));
                 DGPU_CUDA(cudaEventRecord(join[n], p.side_stream));
             }
             if (!jacobi)
