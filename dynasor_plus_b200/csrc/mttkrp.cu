@@ -44,20 +44,6 @@ struct FacPtrs {
     const __nv_bfloat16* Yb[kMaxModes];
 };
 
-__device__ __forceinline__ float4 mul4(float4 a, float4 b) {
-    return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
-}
-__device__ __forceinline__ float4 scale4(float4 a, float s) {
-    return make_float4(s * a.x, s * a.y, s * a.z, s * a.w);
-}
-__device__ __forceinline__ float4 fma4(float4 a, float4 b, float4 c) {
-    return make_float4(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y),
-                       __fmaf_rn(a.z, b.z, c.z), __fmaf_rn(a.w, b.w, c.w));
-}
-__device__ __forceinline__ float4 add4(float4 a, float4 b) {
-    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
-}
-
 template <bool BF>
 __device__ __forceinline__ float4 gather4(const FacPtrs& F, int w, uint32_t row, int Rp, int c4) {
     if constexpr (BF) {
@@ -124,8 +110,10 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
                 const __grid_constant__ FacPtrs F, float* __restrict__ Yhat,
                 int n_rt, int w0_rt, int wl_rt, int Rp, int ld, int rows_contiguous)
 {
+    // the first gathered mode (w0) starts the product by position: only the
+    // target and the fused last mode (wl) need names
     const int n = TN >= 0 ? TN : n_rt;
-    const int w0 = TN >= 0 ? (TN == 0 ? 1 : 0) : w0_rt;
+    (void)w0_rt;
     const int wl = TN >= 0 ? (N == 2 ? -1 : (TN == N - 1 ? N - 2 : N - 1)) : wl_rt;
     constexpr int U = RunBatch<N, V, BF>::U;
     constexpr int NG = 32 / G;                    // groups per warp
