@@ -174,19 +174,31 @@ k_apply_map(const float* __restrict__ Yhat, uint32_t rows, int R, int Rp,
 }
 
 // Partial Grams: grid (chunks, tilesA, tilesB), 32 x 32 output tile per CTA,
-// 4 outputs per thread.  partial[(chunk * R + a) * R + b] (FP64).
+// 16 outputs per thread.  partial[(chunk * R + a) * R + b] (FP64).
 __global__ void __launch_bounds__(kLaThreads)
 k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
                double* __restrict__ partial)
 {
-    __shared__ float sa[64][kGramTile];
-    __shared__ float sb[64][kGramTile];
+    // A block sums one chunk of rows for one (a, b) pair of 32-column tiles.
+    // Thread = (row group g of 4, a-block ta of 8, b-block tb of 8) with a
+    // 4 x 4 register tile: per row it reads two 16-byte vectors from shared
+    // memory for 16 FMAs.  The four row groups take interleaved rows; their
+    // sums are added in a fixed order at the end.
+    static_assert(kLaThreads == 256 && kGramTile == 32, "4 row groups x 8 x 8 threads");
+    __shared__ __align__(16) float sa[64][kGramTile];
+    __shared__ __align__(16) float sb[64][kGramTile];
+    __shared__ float red[3][kGramTile][kGramTile + 1];
     const int a0 = blockIdx.y * kGramTile, b0 = blockIdx.z * kGramTile;
-    const int ta = threadIdx.x >> 3;            // 0..31
-    const int tb = (threadIdx.x & 7) * 4;       // 0..28
+    const bool same = (a0 == b0);
+    const int g = threadIdx.x >> 6, u = threadIdx.x & 63;
+    const int ta = u & 7, tb = u >> 3;
     const uint32_t chunk = (rows + gridDim.x - 1) / gridDim.x;
     const uint32_t r0 = min(rows, blockIdx.x * chunk), r1 = min(rows, r0 + chunk);
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
     for (uint32_t base = r0; base < r1; base += 64) {
         const uint32_t nr = min(64u, r1 - base);
         for (int e = threadIdx.x; e < 64 * kGramTile; e += blockDim.x) {
@@ -195,26 +207,44 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
             if (rr < (int)nr) {
                 const float* y = Y + (size_t)(base + rr) * Rp;
                 if (a0 + cc < R) va = y[a0 + cc];
-                if (b0 + cc < R) vb = y[b0 + cc];
+                if (!same && b0 + cc < R) vb = y[b0 + cc];
             }
             sa[rr][cc] = va;
-            sb[rr][cc] = vb;
+            if (!same) sb[rr][cc] = vb;
         }
         __syncthreads();
-        for (uint32_t rr = 0; rr < nr; ++rr) {
-            const float x = sa[rr][ta];
+        const float (*tb_src)[kGramTile] = same ? sa : sb;
+        for (uint32_t rr = g; rr < nr; rr += 4) {
+            const float4 av = *reinterpret_cast<const float4*>(&sa[rr][4 * ta]);
+            const float4 bv = *reinterpret_cast<const float4*>(&tb_src[rr][4 * tb]);
+            const float x[4] = {av.x, av.y, av.z, av.w};
+            const float y[4] = {bv.x, bv.y, bv.z, bv.w};
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = fmaf(x, sb[rr][tb + q], acc[q]);
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(x[i], y[j], acc[i][j]);
         }
         __syncthreads();
     }
-    const int a = a0 + ta;
-    if (a < R)
+    if (g > 0) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int b = b0 + tb + q;
-            if (b < R) partial[((size_t)blockIdx.x * R + a) * R + b] = (double)acc[q];
-        }
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) red[g - 1][4 * ta + i][4 * tb + j] = acc[i][j];
+    }
+    __syncthreads();
+    if (g == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int a = a0 + 4 * ta + i, b = b0 + 4 * tb + j;
+                const double v = (double)acc[i][j] + (double)red[0][4 * ta + i][4 * tb + j] +
+                                 (double)red[1][4 * ta + i][4 * tb + j] +
+                                 (double)red[2][4 * ta + i][4 * tb + j];
+                if (a < R && b < R) partial[((size_t)blockIdx.x * R + a) * R + b] = v;
+            }
+    }
 }
 
 // Reduce partial Grams; if `normalise`, lambda = sqrt(diag) and the Gram of
