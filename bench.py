@@ -231,6 +231,23 @@ def subsample(dims, vals, idx, k, seed=5):
     return dims, vals[sel], [i[sel] for i in idx]
 
 
+def max_over_ranks(x: float, ws: int, device="cuda") -> float:
+    """The largest of every rank's x (the job's time is its slowest rank)."""
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gnnz_s(nnz_per_rank: int, ws: int, ms_step: float) -> float:
+    """Whole-job throughput of ws replicas, each sweeping nnz_per_rank
+    nonzeros per step, timed by the slowest rank's ms per step."""
+    return ws * nnz_per_rank / (ms_step * 1e-3) / 1e9
+
+
 def run_reference_arm(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
@@ -334,14 +351,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), ws)
     ms_step = ms / args.steps
-    value = ws * nnz / (ms_step * 1e-3) / 1e9
+    value = job_gnnz_s(nnz, ws, ms_step)
 
     # per-kernel timing pass (outside the timed region)
     plan.set_timing(True)
@@ -372,12 +384,7 @@ def main():
         d.check(L.dgpu_mttkrp_sweep_host(plan._h, Yptr, Optr, C.byref(secs)))
     a1.record(stream)
     a1.synchronize()
-    e2e_ms = a0.elapsed_time(a1) / args.steps
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(a0.elapsed_time(a1) / args.steps, ws)
     fbytes = sum(int(dims[n]) * Rp * 4 for n in range(N))
 
     # roofline of the dominant kernel (largest device-time share)
@@ -427,7 +434,7 @@ def main():
         "kernel_times_ms_per_step": {k: v["total_ms"] / 2 for k, v in tim.items() if v["launches"]},
         "kernel_share": {k: v["total_ms"] / total_ms for k, v in tim.items() if v["launches"]},
         "gpu_launches": launches_per_step * args.steps,
-        "e2e": {"value": ws * nnz / (e2e_ms * 1e-3) / 1e9, "unit": "GNNZ/s",
+        "e2e": {"value": job_gnnz_s(nnz, ws, e2e_ms), "unit": "GNNZ/s",
                 "h2d_bytes_per_step": fbytes, "d2h_bytes_per_step": fbytes,
                 "ms_per_step": e2e_ms},
         "clocks": clocks,
