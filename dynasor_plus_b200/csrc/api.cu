@@ -15,6 +15,8 @@
 namespace dgpu {
 int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o);
 int mode_pingpong(Plan& p, int n);
+int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
+                         cudaEvent_t after_mttkrp);
 int mode_ncopy(Plan& p, int n);
 int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& r, double* fit_history);
 int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_result* res,
@@ -355,10 +357,11 @@ int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y, float* const*
         return DGPU_OK;
     }
     // Transfers overlap the mode passes on a second stream: the factors mode 0
-    // gathers go first, Y[0] (first needed by mode 1) streams in while mode 0
-    // runs, and each Yhat[n] streams out while the later modes run.  With
-    // pinned host buffers only the first uploads and the last download are
-    // exposed.
+    // gathers go first (on PingPong plans while mode 0's fiber sort runs),
+    // Y[0] (first needed by mode 1) streams in while mode 0 runs, and each
+    // Yhat[n] streams out as soon as its MTTKRP is done (on PingPong plans
+    // while the remap after it runs).  With pinned host buffers little of
+    // the transfer time is exposed.
     if (!p->copy_stream) DGPU_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
     const int N = p->N;
     std::vector<cudaEvent_t> up(N, nullptr), done(N, nullptr);
@@ -390,12 +393,22 @@ int dgpu_mttkrp_sweep_host(dgpu_plan* plan, const float* const* Y, float* const*
     }
     int rc = DGPU_OK;
     for (int n = 0; n < N && rc == DGPU_OK; ++n) {
-        for (int w = 0; w < N; ++w)
-            if (w != n) DGPU_CUDA(cudaStreamWaitEvent(p->stream, up[w], 0));
         if (n == 0) DGPU_CUDA(cudaEventRecord(e0, p->stream));
-        rc = (p->layout == DGPU_LAYOUT_NCOPY) ? mode_ncopy(*p, n) : mode_pingpong(*p, n);
-        if (rc != DGPU_OK) break;
-        DGPU_CUDA(cudaEventRecord(done[n], p->stream));
+        if (p->layout == DGPU_LAYOUT_NCOPY) {
+            for (int w = 0; w < N; ++w)
+                if (w != n) DGPU_CUDA(cudaStreamWaitEvent(p->stream, up[w], 0));
+            rc = mode_ncopy(*p, n);
+            if (rc != DGPU_OK) break;
+            DGPU_CUDA(cudaEventRecord(done[n], p->stream));
+        } else {
+            // the fiber sort runs while the factors stream in; Yhat[n] streams
+            // out while the remap runs
+            std::vector<cudaEvent_t> waits;
+            for (int w = 0; w < N; ++w)
+                if (w != n) waits.push_back(up[w]);
+            rc = mode_pingpong_staged(*p, n, waits.data(), (int)waits.size(), done[n]);
+            if (rc != DGPU_OK) break;
+        }
         DGPU_CUDA(cudaStreamWaitEvent(p->copy_stream, done[n], 0));
         DGPU_CUDA(cudaMemcpyAsync(Yhat[n], p->Yhat[n], (size_t)p->dims[n] * p->Rp * sizeof(float),
                                   cudaMemcpyDeviceToHost, p->copy_stream));

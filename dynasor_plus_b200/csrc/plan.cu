@@ -799,7 +799,12 @@ int plan_build_dnp(Plan& p, const DnpImage& img, const dgpu_plan_opts& o) {
 
 // One mode of the PingPong sweep: fiber sort (DenseFiber modes), MTTKRP,
 // device remap for mode n+1.  src/dynasor.cpp:352-539.
-int mode_pingpong(Plan& p, int n) {
+// The PingPong mode with two hooks for callers that stream factors in and
+// Yhat out: the MTTKRP waits for `waits` (the fiber sort before it needs no
+// factor), and `after_mttkrp` is recorded once Yhat[n] is complete (the
+// remap after it does not touch Yhat).
+int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
+                         cudaEvent_t after_mttkrp) {
     if (n != p.next_mode) {
         set_error("mttkrp_mode(%d): the slab is remapped for mode %d; modes must run in "
                   "order 0..N-1", n, p.next_mode);
@@ -816,7 +821,9 @@ int mode_pingpong(Plan& p, int n) {
         LaunchTimer t(p, KK_ZERO, (double)yb);
         DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, yb, p.stream));
     }
+    for (int k = 0; k < nwaits; ++k) DGPU_CUDA(cudaStreamWaitEvent(p.stream, waits[k], 0));
     DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
+    if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
     const int nm = (n + 1) % p.N;
     int r = 0;
     DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
@@ -824,6 +831,8 @@ int mode_pingpong(Plan& p, int n) {
     p.next_mode = nm;
     return DGPU_OK;
 }
+
+int mode_pingpong(Plan& p, int n) { return mode_pingpong_staged(p, n, nullptr, 0, nullptr); }
 
 int mode_ncopy(Plan& p, int n) {
     {
