@@ -396,7 +396,7 @@ def main():
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     total_ms = sum(v["total_ms"] for v in tim.values())
     sweep_bytes = sum(v["bytes"] for v in tim.values()) / 2
-    # the north-star algorithmic bytes of a sweep with remap: per mode the
+    # the algorithmic bytes of a sweep with remap: per mode the
     # slab read + the remap write + other factors once + Yhat once
     R = args.rank
     algo = 0.0

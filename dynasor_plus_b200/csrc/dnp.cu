@@ -101,7 +101,7 @@ int check_header(const Header& h, const char* path) {
         return DGPU_ERR_IO;
     }
     if (h.value_bytes != 4 || h.index_bytes != 4) {
-        set_error("dnp: %s: value/index bytes %u/%u, this build uses 4/4", path, h.value_bytes,
+        set_error("dnp: %s: value/index bytes %u/%u, only 4/4 is supported", path, h.value_bytes,
                   h.index_bytes);
         return DGPU_ERR_IO;
     }

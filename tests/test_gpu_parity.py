@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 SWEEP_CASES = sorted(os.path.basename(p) for p in glob.glob(os.path.join(GOLDEN, "ref_*.npz"))
                      if "cpals" not in p)
-TOL_FP32 = 1e-5          # north-star bound vs the reference MTTKRP (FP32)
+TOL_FP32 = 1e-5          # bound vs the reference MTTKRP (FP32)
 TOL_BF16 = 2e-2          # BF16 gathers (8-bit mantissa) vs FP64
 
 
@@ -171,6 +171,40 @@ def test_bf16_gathers_close_to_fp64(bindings):
         assert err <= TOL_BF16, (n, err)
         v, ix = o.slab()
         _assert_slab(p, v, ix, f"mode {n}")
+
+
+def _round_bf16(y):
+    """FP32 -> BF16 -> FP32 with round-to-nearest-even (finite inputs)."""
+    b = np.ascontiguousarray(y, np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("dims", [(4000, 900, 300), (3000, 700, 200, 60)])
+@pytest.mark.parametrize("R", [16, 32, 48, 64, 128])
+def test_bf16_rowrun_exact_on_rounded_factors(bindings, dims, R):
+    """The row-run kernel with BF16 gathers (every lane-group shape, rank
+    tiles at R = 128): FP32 products of the BF16-rounded factors, so it
+    meets the FP32 bound against an FP64 MTTKRP of those rounded factors."""
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.zipf(dims, draws=60000, s=1.1, seed=43 + R)
+    N = len(dims)
+    p = _plan(dims, vals, idx, 8, R, precision="bf16", accum="rowrun")
+    rng = np.random.default_rng(R)
+    Y = []
+    for n in range(N):
+        y = np.zeros((int(dims[n]), p.Rp), np.float32)
+        y[:, :R] = rng.uniform(-1, 1, (int(dims[n]), R))
+        Y.append(y)
+        p.set_factor(n, y)
+    Yb = [_round_bf16(y) for y in Y]
+    for n in range(N):
+        p.process(n)
+        y64 = bindings.mttkrp_f64(vals, idx, n, Yb, R, int(dims[n]))
+        got = p.yhat(n)
+        assert rel_fro(got[:, :R], y64[:, :R]) <= TOL_FP32, (n, rel_fro(got[:, :R], y64[:, :R]))
+        assert np.all(got[:, R:] == 0)
+    p.close()
 
 
 def test_out_of_order_mode_is_rejected():
