@@ -175,6 +175,9 @@ struct Plan {
     bool         own_stream = false;
     cudaStream_t copy_stream = nullptr;         // host transfers overlapping the sweep
     cudaStream_t side_stream = nullptr;         // CP-ALS solves overlapping the MTTKRP
+    cudaStream_t ovl_stream = nullptr;          // PingPong: MTTKRP beside the remap
+    cudaEvent_t  ovl_fork = nullptr, ovl_join = nullptr;
+    int          overlap = 1;                   // 0: MTTKRP then remap on the plan stream
     Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for

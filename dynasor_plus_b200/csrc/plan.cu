@@ -191,6 +191,9 @@ Plan::~Plan() {
     for (auto e : cp_join) cudaEventDestroy(e);
     if (copy_stream) { cudaStreamSynchronize(copy_stream); cudaStreamDestroy(copy_stream); }
     if (side_stream) { cudaStreamSynchronize(side_stream); cudaStreamDestroy(side_stream); }
+    if (ovl_stream) { cudaStreamSynchronize(ovl_stream); cudaStreamDestroy(ovl_stream); }
+    if (ovl_fork) cudaEventDestroy(ovl_fork);
+    if (ovl_join) cudaEventDestroy(ovl_join);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -379,6 +382,7 @@ static int plan_init(Plan& p, int N, uint64_t nnz, const uint32_t* dims, const d
     if (const char* e = std::getenv("DGPU_SORT_DIGIT_BITS")) p.sort_digit_bits = std::atoi(e);
     if (const char* e = std::getenv("DGPU_FIBER_DIGIT_BITS")) p.fiber_digit_bits = std::atoi(e);
     if (const char* e = std::getenv("DGPU_RANK_TILE")) p.rank_tile = std::atoi(e);
+    if (const char* e = std::getenv("DGPU_OVERLAP")) p.overlap = std::atoi(e);
     for (int n = 0; n < N; ++n) p.dims[n] = dims[n];
     return DGPU_OK;
 }
@@ -822,11 +826,44 @@ int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
         DGPU_CUDA(cudaMemsetAsync(p.Yhat[n], 0, yb, p.stream));
     }
     for (int k = 0; k < nwaits; ++k) DGPU_CUDA(cudaStreamWaitEvent(p.stream, waits[k], 0));
-    DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
-    if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
     const int nm = (n + 1) % p.N;
     int r = 0;
-    DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
+    // overlap needs a one-pass remap: a second LSD pass would write back
+    // into the slab the MTTKRP is reading
+    const int digit = std::max(1, std::min(kDigitBits, p.sort_digit_bits));
+    const bool one_pass = (uint64_t)p.K[nm] <= ((uint64_t)1 << digit);
+    if (p.overlap == 0 || p.timing || !one_pass) {
+        DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
+        if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
+        DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
+    } else {
+        // The MTTKRP and the remap both only read the live slab (the remap
+        // writes the other one), so the MTTKRP runs on ovl_stream beside the
+        // remap on the plan stream, joined before returning.  The MTTKRP is
+        // launched first; the remap's CTAs start as its last CTAs drain
+        // (each kernel fills the SMs' registers, so that tail is the overlap;
+        // measured 9.72 -> 9.61 ms per sweep on the 64.7M-nonzero tensor).
+        if (!p.ovl_stream) {
+            DGPU_CUDA(cudaStreamCreateWithFlags(&p.ovl_stream, cudaStreamNonBlocking));
+            DGPU_CUDA(cudaEventCreateWithFlags(&p.ovl_fork, cudaEventDisableTiming));
+            DGPU_CUDA(cudaEventCreateWithFlags(&p.ovl_join, cudaEventDisableTiming));
+        }
+        DGPU_CUDA(cudaEventRecord(p.ovl_fork, p.stream));
+        DGPU_CUDA(cudaStreamWaitEvent(p.ovl_stream, p.ovl_fork, 0));
+        const cudaStream_t main = p.stream;
+        struct Restore {
+            Plan& p;
+            cudaStream_t s;
+            ~Restore() { p.stream = s; }
+        } restore{p, main};
+        p.stream = p.ovl_stream;
+        DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
+        if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
+        DGPU_CUDA(cudaEventRecord(p.ovl_join, p.stream));
+        p.stream = main;
+        DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
+        DGPU_CUDA(cudaStreamWaitEvent(main, p.ovl_join, 0));
+    }
     p.cur = r;
     p.next_mode = nm;
     return DGPU_OK;
