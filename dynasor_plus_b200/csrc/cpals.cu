@@ -24,6 +24,7 @@
 //                       linalg.cpp:365; this keeps FP64 throughout).
 //  Grams are kept in FP64 between modes.
 // ============================================================================
+#include <functional>
 #include "dgpu_internal.h"
 #include "la_warp.cuh"
 
@@ -40,6 +41,7 @@
 namespace dgpu {
 
 int mode_pingpong(Plan& p, int n);
+int mode_pingpong_then(Plan& p, int n, const std::function<int()>& after);
 int mode_ncopy(Plan& p, int n);
 
 namespace {
@@ -968,7 +970,10 @@ struct CpSession {
             // before this one)
             const bool ovl = !jacobi;
             if (ovl) {
-                DGPU_CUDA(cudaEventRecord(fork[n], p.stream));
+                // the previous update may still run on the PingPong overlap
+                // stream: fork from there
+                const cudaStream_t from = p.ovl_pending ? p.ovl_stream : p.stream;
+                DGPU_CUDA(cudaEventRecord(fork[n], from));
                 DGPU_CUDA(cudaStreamWaitEvent(p.side_stream, fork[n], 0));
                 if (small_mode(p, n))
                     DGPU_TRY(launch_small_solve(p, L, n, o.solve_fp64, o.ridge, p.side_stream));
@@ -976,14 +981,28 @@ struct CpSession {
                     DGPU_TRY(launch_large_solve(p, L, n, o.solve_fp64, o.ridge, p.side_stream));
                 DGPU_CUDA(cudaEventRecord(join[n], p.side_stream));
             }
-            if (!jacobi)
-                DGPU_TRY(p.layout == DGPU_LAYOUT_NCOPY ? mode_ncopy(p, n) : mode_pingpong(p, n));
-            DGPU_CUDA(rec(1 + 2 * n));
-            if (ovl) DGPU_CUDA(cudaStreamWaitEvent(p.stream, join[n], 0));
-            DGPU_TRY(update_mode(p, L, n, o.solve_fp64, o.ridge, n == p.N - 1, tn2, &fit_done,
-                                 ovl ? L.Wd : nullptr));
-            DGPU_CUDA(rec(2 + 2 * n));
+            // the factor update (on the stream that ran the MTTKRP)
+            auto update = [&]() -> int {
+                DGPU_CUDA(rec(1 + 2 * n));
+                if (ovl) DGPU_CUDA(cudaStreamWaitEvent(p.stream, join[n], 0));
+                DGPU_TRY(update_mode(p, L, n, o.solve_fp64, o.ridge, n == p.N - 1, tn2, &fit_done,
+                                     ovl ? L.Wd : nullptr));
+                DGPU_CUDA(rec(2 + 2 * n));
+                return DGPU_OK;
+            };
+            if (jacobi) {
+                DGPU_TRY(update());
+            } else if (p.layout == DGPU_LAYOUT_NCOPY) {
+                DGPU_TRY(mode_ncopy(p, n));
+                DGPU_TRY(update());
+            } else {
+                // PingPong: the update needs this mode's Yhat, not the
+                // remapped slab, so it runs beside the remap and the next
+                // mode's fiber sort
+                DGPU_TRY(mode_pingpong_then(p, n, update));
+            }
         }
+        DGPU_TRY(pingpong_drain(p));
         if (!fit_done) {
             const int nblk = (int)grid_for((size_t)p.dims[p.N - 1] * p.Rp, kGramChunks);
             k_fit<<<1, 1024, 0, p.stream>>>(L.Gd, p.N, p.R, L.lam64, L.dot, nblk, tn2, L.fitout);

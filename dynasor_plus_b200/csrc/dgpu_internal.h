@@ -176,7 +176,8 @@ struct Plan {
     cudaStream_t copy_stream = nullptr;         // host transfers overlapping the sweep
     cudaStream_t side_stream = nullptr;         // CP-ALS solves overlapping the MTTKRP
     cudaStream_t ovl_stream = nullptr;          // PingPong: MTTKRP beside the remap
-    cudaEvent_t  ovl_fork = nullptr, ovl_join = nullptr;
+    cudaEvent_t  ovl_fork = nullptr, ovl_join = nullptr, ovl_tail = nullptr;
+    bool         ovl_pending = false;           // work after ovl_tail's record not yet joined
     int          overlap = 1;                   // 0: MTTKRP then remap on the plan stream
     Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
     int          cur = 0;                       // PingPong: live slab index
@@ -250,6 +251,10 @@ int timing_collect(Plan& p);
 // waits that gave up, out-of-range keys); a raised flag is cleared and
 // reported as DGPU_ERR_DEVICE.
 int sync_checked(Plan& p);
+
+// PingPong: makes the plan stream wait for work that a chained mode left on
+// ovl_stream (plan.cu, mode_pingpong_then).
+int pingpong_drain(Plan& p);
 
 // ---- Morton layout (morton.cu) -------------------------------------------
 // Key bit positions of each mode's index bits, LSB first: decoding is pext

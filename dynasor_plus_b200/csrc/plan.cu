@@ -20,6 +20,7 @@
 #include "dgpu_internal.h"
 
 #include <algorithm>
+#include <functional>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -194,6 +195,7 @@ Plan::~Plan() {
     if (ovl_stream) { cudaStreamSynchronize(ovl_stream); cudaStreamDestroy(ovl_stream); }
     if (ovl_fork) cudaEventDestroy(ovl_fork);
     if (ovl_join) cudaEventDestroy(ovl_join);
+    if (ovl_tail) cudaEventDestroy(ovl_tail);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -807,8 +809,11 @@ int plan_build_dnp(Plan& p, const DnpImage& img, const dgpu_plan_opts& o) {
 // Yhat out: the MTTKRP waits for `waits` (the fiber sort before it needs no
 // factor), and `after_mttkrp` is recorded once Yhat[n] is complete (the
 // remap after it does not touch Yhat).
-int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
-                         cudaEvent_t after_mttkrp) {
+// One PingPong mode.  `after` (optional) enqueues work that needs this
+// mode's Yhat but not the remapped slab (a CP-ALS factor update): it runs
+// right after the MTTKRP on the MTTKRP's stream.
+static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
+                              cudaEvent_t after_mttkrp, const std::function<int()>* after) {
     if (n != p.next_mode) {
         set_error("mttkrp_mode(%d): the slab is remapped for mode %d; modes must run in "
                   "order 0..N-1", n, p.next_mode);
@@ -833,20 +838,26 @@ int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
     const int digit = std::max(1, std::min(kDigitBits, p.sort_digit_bits));
     const bool one_pass = (uint64_t)p.K[nm] <= ((uint64_t)1 << digit);
     if (p.overlap == 0 || p.timing || !one_pass) {
+        DGPU_TRY(pingpong_drain(p));
         DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
         if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
+        if (after) DGPU_TRY((*after)());
         DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
     } else {
         // The MTTKRP and the remap both only read the live slab (the remap
         // writes the other one), so the MTTKRP runs on ovl_stream beside the
-        // remap on the plan stream, joined before returning.  The MTTKRP is
-        // launched first; the remap's CTAs start as its last CTAs drain
-        // (each kernel fills the SMs' registers, so that tail is the overlap;
-        // measured 9.72 -> 9.61 ms per sweep on the 64.7M-nonzero tensor).
+        // remap on the plan stream.  The MTTKRP is launched first; the
+        // remap's CTAs start as its last CTAs drain (each kernel fills the
+        // SMs' registers, so that tail is the overlap; measured 9.72 -> 9.61
+        // ms per sweep on the 64.7M-nonzero tensor).  The plan stream waits
+        // for the MTTKRP only (the next mode's fiber sort overwrites the
+        // slab it read); `after` stays on ovl_stream, beside the remap and
+        // the next fiber sort, until pingpong_drain.
         if (!p.ovl_stream) {
             DGPU_CUDA(cudaStreamCreateWithFlags(&p.ovl_stream, cudaStreamNonBlocking));
             DGPU_CUDA(cudaEventCreateWithFlags(&p.ovl_fork, cudaEventDisableTiming));
             DGPU_CUDA(cudaEventCreateWithFlags(&p.ovl_join, cudaEventDisableTiming));
+            DGPU_CUDA(cudaEventCreateWithFlags(&p.ovl_tail, cudaEventDisableTiming));
         }
         DGPU_CUDA(cudaEventRecord(p.ovl_fork, p.stream));
         DGPU_CUDA(cudaStreamWaitEvent(p.ovl_stream, p.ovl_fork, 0));
@@ -860,6 +871,11 @@ int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
         DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
         if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
         DGPU_CUDA(cudaEventRecord(p.ovl_join, p.stream));
+        if (after) {
+            DGPU_TRY((*after)());
+            DGPU_CUDA(cudaEventRecord(p.ovl_tail, p.stream));
+            p.ovl_pending = true;
+        }
         p.stream = main;
         DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
         DGPU_CUDA(cudaStreamWaitEvent(main, p.ovl_join, 0));
@@ -867,6 +883,23 @@ int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
     p.cur = r;
     p.next_mode = nm;
     return DGPU_OK;
+}
+
+int pingpong_drain(Plan& p) {
+    if (p.ovl_pending) {
+        DGPU_CUDA(cudaStreamWaitEvent(p.stream, p.ovl_tail, 0));
+        p.ovl_pending = false;
+    }
+    return DGPU_OK;
+}
+
+int mode_pingpong_staged(Plan& p, int n, const cudaEvent_t* waits, int nwaits,
+                         cudaEvent_t after_mttkrp) {
+    return mode_pingpong_impl(p, n, waits, nwaits, after_mttkrp, nullptr);
+}
+
+int mode_pingpong_then(Plan& p, int n, const std::function<int()>& after) {
+    return mode_pingpong_impl(p, n, nullptr, 0, nullptr, &after);
 }
 
 int mode_pingpong(Plan& p, int n) { return mode_pingpong_staged(p, n, nullptr, 0, nullptr); }

@@ -29,7 +29,11 @@ def test_fit_trajectory_matches_reference(solve_fp64):
     assert np.max(np.abs(r["fit_history"] - g["fit"])) < FIT_TOL
 
 
-def test_fit_and_factors_match_fp64_oracle(bindings):
+@pytest.mark.parametrize("overlap", ["1", "0"])
+def test_fit_and_factors_match_fp64_oracle(bindings, overlap, monkeypatch):
+    # overlap "1" (default): each PingPong factor update runs on a second
+    # stream beside the remap and the next fiber sort; "0": one stream
+    monkeypatch.setenv("DGPU_OVERLAP", overlap)
     g, dims, idx, p = _golden_plan()
     it, tol, R = int(g["iters"]), float(g["tol"]), int(g["R"])
     r = p.cpals(max_iters=it, tol=tol, seed=42)
@@ -99,10 +103,13 @@ def test_graph_replay_matches_eager_iterations(layout, kernel):
         assert rel_fro(b, a) < (1e-4 if kernel == "jacobi" else 1e-5)
 
 
+@pytest.mark.parametrize("overlap", ["1", "0"])
 @pytest.mark.parametrize("solve_fp64", [True, False])
-def test_large_and_small_mode_updates_match_fp64_oracle(bindings, solve_fp64):
+def test_large_and_small_mode_updates_match_fp64_oracle(bindings, solve_fp64, overlap, monkeypatch):
     """Mode 0 (40,000 rows x rank 16) takes the multi-kernel factor update,
-    modes 1-2 the single-CTA one; the trajectory follows the FP64 oracle."""
+    modes 1-2 the single-CTA one; the trajectory follows the FP64 oracle
+    with the PingPong updates beside the remaps and on one stream."""
+    monkeypatch.setenv("DGPU_OVERLAP", overlap)
     import dynasor_plus_b200 as d
     from dynasor_plus_b200 import synth
     dims, vals, idx = synth.cp_truth((40_000, 300, 200), 200_000, 5, 0.01, seed=7)
