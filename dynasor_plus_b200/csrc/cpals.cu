@@ -175,6 +175,160 @@ k_apply_map(const float* __restrict__ Yhat, uint32_t rows, int R, int Rp,
     }
 }
 
+// The same map for Rp = RP in {16, 32}: lane c of a warp (c = lane % RP)
+// owns output column c with column c of W in registers; a warp stages 8
+// rows of Yhat (converted to Real) in its own shared-memory slice and reads
+// them back as broadcasts, so each Yhat entry is converted once and each
+// loaded pair of entries feeds a multiply-add in every lane.  The next 8
+// rows are loaded while the current ones are multiplied.  Each output is the
+// same k-ordered fused multiply-add chain as in k_apply_map.
+constexpr int kMapRows = 8;                    // rows a warp stages at a time
+template <typename Real, int RP>
+__global__ void __launch_bounds__(kLaThreads, 2)
+k_apply_map_lanes(const float* __restrict__ Yhat, uint32_t rows, int R,
+                  const Real* __restrict__ W, float* __restrict__ Y)
+{
+    static_assert(RP == 16 || RP == 32, "one or two rows per warp pass");
+    constexpr int RW = 32 / RP;                          // rows per warp pass
+    constexpr int V4 = kMapRows * RP / 4 / 32;            // float4 loads per lane per block
+    __shared__ __align__(16) Real hs[kLaThreads / 32][kMapRows][RP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = lane % RP, sub = lane / RP;
+    Real w[RP];
+#pragma unroll
+    for (int k = 0; k < RP; ++k) w[k] = (k < R && c < R) ? W[(size_t)k * R + c] : (Real)0;
+    const uint32_t nblocks = (rows + kMapRows - 1) / kMapRows;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const float4* src = reinterpret_cast<const float4*>(Yhat);
+    const size_t n4 = (size_t)rows * RP / 4;
+    float4 pf[V4];
+    auto load = [&](uint32_t b) {
+#pragma unroll
+        for (int v = 0; v < V4; ++v) {
+            const size_t q = (size_t)b * (kMapRows * RP / 4) + v * 32 + lane;
+            pf[v] = q < n4 ? __ldg(src + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    uint32_t b = gw;
+    if (b < nblocks) load(b);
+    for (; b < nblocks; b += nw) {
+        Real* hw = &hs[warp][0][0];
+#pragma unroll
+        for (int v = 0; v < V4; ++v) {
+            const int e = (v * 32 + lane) * 4;               // element within the block
+            hw[e] = (Real)pf[v].x; hw[e + 1] = (Real)pf[v].y;
+            hw[e + 2] = (Real)pf[v].z; hw[e + 3] = (Real)pf[v].w;
+        }
+        __syncwarp();
+        if (b + nw < nblocks) load(b + nw);
+#pragma unroll
+        for (int r0 = 0; r0 < kMapRows; r0 += RW) {
+            const int r = r0 + sub;
+            const Real* h = &hs[warp][r][0];
+            Real acc = 0;
+#pragma unroll
+            for (int k = 0; k < RP; k += 2) {
+                Real h0, h1;
+                if constexpr (sizeof(Real) == 8) {
+                    const double2 hv = *reinterpret_cast<const double2*>(h + k);
+                    h0 = hv.x; h1 = hv.y;
+                } else {
+                    const float2 hv = *reinterpret_cast<const float2*>(h + k);
+                    h0 = hv.x; h1 = hv.y;
+                }
+                if constexpr (sizeof(Real) == 8) {
+                    if (k < R) acc = fma(h0, w[k], acc);
+                    if (k + 1 < R) acc = fma(h1, w[k + 1], acc);
+                } else {
+                    if (k < R) acc = fmaf(h0, w[k], acc);
+                    if (k + 1 < R) acc = fmaf(h1, w[k + 1], acc);
+                }
+            }
+            const uint32_t i = b * kMapRows + r;
+            if (i < rows) Y[(size_t)i * RP + c] = c < R ? (float)acc : 0.f;
+        }
+        __syncwarp();
+    }
+}
+
+// FP64 map on the FP64 tensor pipe (mma.sync m8n8k4 .f64) for Rp = RP in
+// {16, 32}: a warp multiplies blocks of 8 rows, Y(8 x RP) = Yhat(8 x RP) *
+// W(RP x RP), as RP/4 k-steps x RP/8 column tiles.  W's fragments stay in
+// registers (thread (g, t) = (lane / 4, lane % 4) holds W[4s + t][8j + g]);
+// the 8 rows are staged in a padded shared-memory slice (row stride RP + 4
+// floats: the A-fragment reads A[g][4s + t] fall in 32 distinct banks) and
+// converted to FP64 on the way into the fragments.  The next block is
+// loaded while the current one is multiplied.
+template <int RP>
+__global__ void __launch_bounds__(kLaThreads, 2)
+k_apply_map_dmma(const float* __restrict__ Yhat, uint32_t rows, int R,
+                 const double* __restrict__ W, float* __restrict__ Y)
+{
+    static_assert(RP == 16 || RP == 32, "two or four column tiles");
+    constexpr int NT = RP / 8, KS = RP / 4, LD = RP + 4;
+    constexpr int V4 = kMapRows * RP / 4 / 32;            // float4 loads per lane per block
+    __shared__ __align__(16) float hs[kLaThreads / 32][kMapRows][LD];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    double b[KS][NT];
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const int k = 4 * ks + t, c = 8 * j + g;
+            b[ks][j] = (k < R && c < R) ? W[(size_t)k * R + c] : 0.0;
+        }
+    const uint32_t nblocks = (rows + kMapRows - 1) / kMapRows;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const float4* src = reinterpret_cast<const float4*>(Yhat);
+    const size_t n4 = (size_t)rows * RP / 4;
+    float4 pf[V4];
+    auto load = [&](uint32_t blk) {
+#pragma unroll
+        for (int v = 0; v < V4; ++v) {
+            const size_t q = (size_t)blk * (kMapRows * RP / 4) + v * 32 + lane;
+            pf[v] = q < n4 ? __ldg(src + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    uint32_t blk = gw;
+    if (blk < nblocks) load(blk);
+    for (; blk < nblocks; blk += nw) {
+#pragma unroll
+        for (int v = 0; v < V4; ++v) {
+            const int e = (v * 32 + lane) * 4;
+            *reinterpret_cast<float4*>(&hs[warp][e / RP][e % RP]) = pf[v];
+        }
+        __syncwarp();
+        if (blk + nw < nblocks) load(blk + nw);
+        double a[KS];
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) a[ks] = (double)hs[warp][g][4 * ks + t];
+        double acc[NT][2];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                             : "+d"(acc[j][0]), "+d"(acc[j][1]) : "d"(a[ks]), "d"(b[ks][j]));
+        const uint32_t i = blk * kMapRows + g;
+        if (i < rows) {
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                const int c = 8 * j + 2 * t;
+                float2 o;
+                o.x = c < R ? (float)acc[j][0] : 0.f;
+                o.y = c + 1 < R ? (float)acc[j][1] : 0.f;
+                *reinterpret_cast<float2*>(Y + (size_t)i * RP + c) = o;
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Partial Grams: grid (chunks, tilesA, tilesB), 32 x 32 output tile per CTA,
 // 16 outputs per thread.  partial[(chunk * R + a) * R + b] (FP64).
 __global__ void __launch_bounds__(kLaThreads)
@@ -201,20 +355,38 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    for (uint32_t base = r0; base < r1; base += 64) {
+    // the next 64 rows are loaded into registers while the current ones are
+    // multiplied (all of a thread's loads in flight at once)
+    constexpr int PER = 64 * kGramTile / kLaThreads;
+    float na[PER], nb[PER];
+    auto fetch = [&](uint32_t base) {
         const uint32_t nr = min(64u, r1 - base);
-        for (int e = threadIdx.x; e < 64 * kGramTile; e += blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int e = threadIdx.x + j * kLaThreads;
             const int rr = e / kGramTile, cc = e % kGramTile;
             float va = 0.f, vb = 0.f;
             if (rr < (int)nr) {
                 const float* y = Y + (size_t)(base + rr) * Rp;
-                if (a0 + cc < R) va = y[a0 + cc];
-                if (!same && b0 + cc < R) vb = y[b0 + cc];
+                if (a0 + cc < R) va = __ldg(y + a0 + cc);
+                if (!same && b0 + cc < R) vb = __ldg(y + b0 + cc);
             }
-            sa[rr][cc] = va;
-            if (!same) sb[rr][cc] = vb;
+            na[j] = va;
+            nb[j] = vb;
+        }
+    };
+    if (r0 < r1) fetch(r0);
+    for (uint32_t base = r0; base < r1; base += 64) {
+        const uint32_t nr = min(64u, r1 - base);
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            const int e = threadIdx.x + j * kLaThreads;
+            const int rr = e / kGramTile, cc = e % kGramTile;
+            sa[rr][cc] = na[j];
+            if (!same) sb[rr][cc] = nb[j];
         }
         __syncthreads();
+        if (base + 64 < r1) fetch(base + 64);
         const float (*tb_src)[kGramTile] = same ? sa : sb;
         for (uint32_t rr = g; rr < nr; rr += 4) {
             const float4 av = *reinterpret_cast<const float4*>(&sa[rr][4 * ta]);
@@ -249,6 +421,34 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
     }
 }
 
+// Sums the `chunks` partial Grams into partial[0 .. RR) (in place): a CTA
+// takes 32 entries, its 8 warps take 8 consecutive runs of chunks and the
+// 8 run sums are added in run order, so the result does not depend on
+// timing.  Spreading the 2.4 MB of partials of a large mode over many SMs
+// replaces one CTA reading all of them.
+__global__ void __launch_bounds__(256)
+k_reduce_partials(double* __restrict__ partial, int chunks, int RR)
+{
+    __shared__ double run[8][32];
+    const int el = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int e = blockIdx.x * 32 + el;
+    const int per = (chunks + 7) / 8;
+    const int c0 = min(chunks, w * per), c1 = min(chunks, c0 + per);
+    double s = 0.0;
+    if (e < RR) {
+#pragma unroll 4
+        for (int c = c0; c < c1; ++c) s += partial[(size_t)c * RR + e];
+    }
+    run[w][el] = s;
+    __syncthreads();
+    if (w == 0 && e < RR) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t += run[k][el];
+        partial[e] = t;
+    }
+}
+
 // Reduce partial Grams; if `normalise`, lambda = sqrt(diag) and the Gram of
 // the column-normalised factor is stored; else the raw Gram.
 __global__ void __launch_bounds__(1024)
@@ -259,6 +459,8 @@ k_finalize_mode(const double* __restrict__ partial, int chunks, int R, int ldo, 
     const size_t RR = (size_t)R * R;
     for (size_t e = threadIdx.x; e < RR; e += blockDim.x) {
         double s = 0;
+        // in chunk order; unrolled so that the loads are in flight together
+#pragma unroll 8
         for (int c = 0; c < chunks; ++c) s += partial[(size_t)c * RR + e];
         Gd_n[e] = s;
     }
@@ -299,7 +501,48 @@ k_scale_cols(float* __restrict__ Y, const float* __restrict__ Yhat, uint32_t row
     const size_t total = (size_t)rows * Rp;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (Yhat && stride % Rp == 0) {
+    const int C4 = Rp >> 2;
+    if ((Rp & 3) == 0 && stride % C4 == 0) {
+        // float4 per thread, every float4 this thread visits in one group of
+        // four columns; four float4 of Y (and of Yhat) in flight at once
+        constexpr int U = 4;
+        const int c0 = (int)(first % C4) * 4;
+        float inv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) inv[j] = c0 + j < R ? invs[c0 + j] : 0.f;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        float4* Y4 = reinterpret_cast<float4*>(Y);
+        const float4* H4 = reinterpret_cast<const float4*>(Yhat);
+        const size_t total4 = total >> 2;
+        for (size_t q = first; q < total4; q += U * stride) {
+            float4 y[U], h[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const size_t qq = q + u * stride;
+                y[u] = qq < total4 ? Y4[qq] : make_float4(0.f, 0.f, 0.f, 0.f);
+                h[u] = (Yhat && qq < total4) ? __ldg(H4 + qq) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const size_t qq = q + u * stride;
+                if (qq >= total4) break;
+                const float4 v = make_float4(y[u].x * inv[0], y[u].y * inv[1], y[u].z * inv[2],
+                                             y[u].w * inv[3]);
+                Y4[qq] = v;
+                if (Yhat) {
+                    acc[0] += (double)v.x * (double)h[u].x;
+                    acc[1] += (double)v.y * (double)h[u].y;
+                    acc[2] += (double)v.z * (double)h[u].z;
+                    acc[3] += (double)v.w * (double)h[u].w;
+                }
+            }
+        }
+        if (Yhat) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (c0 + j < R) atomicAdd(&sdot[c0 + j], acc[j]);
+        }
+    } else if (Yhat && stride % Rp == 0) {
         // every element this thread visits is in one column: one atomic
         const int c = (int)(first % Rp);
         double acc = 0.0;
@@ -679,7 +922,12 @@ int gram_into(Plan& p, const LaLayout& L, int n, int normalise) {
     dim3 grid(chunks, tiles, tiles);
     k_gram_partial<<<grid, kLaThreads, 0, p.stream>>>(p.Y[n], p.dims[n], p.R, p.Rp, L.partial);
     const size_t RR = (size_t)p.R * p.R;
-    k_finalize_mode<<<1, 1024, 0, p.stream>>>(L.partial, chunks, p.R, p.R, normalise,
+    int fin_chunks = chunks;
+    if (chunks > 8) {
+        k_reduce_partials<<<(unsigned)((RR + 31) / 32), 256, 0, p.stream>>>(L.partial, chunks, (int)RR);
+        fin_chunks = 1;
+    }
+    k_finalize_mode<<<1, 1024, 0, p.stream>>>(L.partial, fin_chunks, p.R, p.R, normalise,
                                               L.Gd + (size_t)n * RR, L.G32 + (size_t)n * RR,
                                               p.lambda, L.lam64);
     DGPU_CUDA(cudaGetLastError());
@@ -765,7 +1013,17 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
         return DGPU_OK;
     }
     if (!Wpre) DGPU_TRY(launch_large_solve(p, L, n, solve_fp64, ridge, p.stream));
-    if (solve_fp64) {
+    if (p.Rp == 16 || p.Rp == 32) {
+        const unsigned gm = grid_for((size_t)p.dims[n] * p.Rp / 4);
+        if (solve_fp64 && p.Rp == 16)
+            k_apply_map_dmma<16><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.Wd, p.Y[n]);
+        else if (solve_fp64)
+            k_apply_map_dmma<32><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.Wd, p.Y[n]);
+        else if (p.Rp == 16)
+            k_apply_map_lanes<float, 16><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.W32, p.Y[n]);
+        else
+            k_apply_map_lanes<float, 32><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.W32, p.Y[n]);
+    } else if (solve_fp64) {
         const size_t sm = RR * sizeof(double);
         if (sm > 48 * 1024)
             DGPU_CUDA(cudaFuncSetAttribute(k_apply_map<double>,

@@ -103,17 +103,19 @@ def test_graph_replay_matches_eager_iterations(layout, kernel):
         assert rel_fro(b, a) < (1e-4 if kernel == "jacobi" else 1e-5)
 
 
+@pytest.mark.parametrize("R", [16, 32, 48])
 @pytest.mark.parametrize("overlap", ["1", "0"])
 @pytest.mark.parametrize("solve_fp64", [True, False])
-def test_large_and_small_mode_updates_match_fp64_oracle(bindings, solve_fp64, overlap, monkeypatch):
-    """Mode 0 (40,000 rows x rank 16) takes the multi-kernel factor update,
-    modes 1-2 the single-CTA one; the trajectory follows the FP64 oracle
-    with the PingPong updates beside the remaps and on one stream."""
+def test_large_and_small_mode_updates_match_fp64_oracle(bindings, solve_fp64, overlap, R, monkeypatch):
+    """Mode 0 (40,000 rows) takes the multi-kernel factor update (the FP64
+    map on the tensor pipe at Rp 16 and 32, the shared-memory map at Rp 48),
+    mode 2 the single-CTA one; the trajectory follows the FP64 oracle with
+    the PingPong updates beside the remaps and on one stream."""
     monkeypatch.setenv("DGPU_OVERLAP", overlap)
     import dynasor_plus_b200 as d
     from dynasor_plus_b200 import synth
     dims, vals, idx = synth.cp_truth((40_000, 300, 200), 200_000, 5, 0.01, seed=7)
-    R, it = 16, 6
+    it = 6
     p = d.Plan(dims, vals, idx, threads=8, rank=R)
     r = p.cpals(max_iters=it, tol=0.0, seed=42, solve_fp64=solve_fp64)
     fit64, Y64, lam64 = bindings.cpals_f64(dims, vals, idx, R, it, 0.0, seed=42)
