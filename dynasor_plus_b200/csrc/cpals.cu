@@ -329,9 +329,23 @@ k_apply_map_dmma(const float* __restrict__ Yhat, uint32_t rows, int R,
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+                 :: "r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(src),
+                    "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
+// Rows a partial-Gram CTA stages per step, and steps in flight.
+constexpr int kGramRows = 64;
+constexpr int kGramStages = 4;
+constexpr size_t kGramSmem = 2 * (size_t)kGramStages * kGramRows * kGramTile * sizeof(float);
+
 // Partial Grams: grid (chunks, tilesA, tilesB), 32 x 32 output tile per CTA,
 // 16 outputs per thread.  partial[(chunk * R + a) * R + b] (FP64).
-__global__ void __launch_bounds__(kLaThreads)
+__global__ void __launch_bounds__(kLaThreads, 2)
 k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
                double* __restrict__ partial)
 {
@@ -339,58 +353,66 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
     // Thread = (row group g of 4, a-block ta of 8, b-block tb of 8) with a
     // 4 x 4 register tile: per row it reads two 16-byte vectors from shared
     // memory for 16 FMAs.  The four row groups take interleaved rows; their
-    // sums are added in a fixed order at the end.
+    // sums are added in a fixed order at the end.  Rows stream into a
+    // kGramStages-deep ring of shared-memory stages with 16-byte cp.async
+    // copies (zero fill past the chunk and past Rp), so three steps of loads
+    // are in flight while one is multiplied.  Columns >= R only reach Gram
+    // entries that are not stored.
     static_assert(kLaThreads == 256 && kGramTile == 32, "4 row groups x 8 x 8 threads");
-    __shared__ __align__(16) float sa[64][kGramTile];
-    __shared__ __align__(16) float sb[64][kGramTile];
-    __shared__ float red[3][kGramTile][kGramTile + 1];
+    extern __shared__ __align__(16) float gsm[];
+    typedef float Stage[kGramRows][kGramTile];
+    Stage* sa = reinterpret_cast<Stage*>(gsm);
+    Stage* sb = sa + kGramStages;
     const int a0 = blockIdx.y * kGramTile, b0 = blockIdx.z * kGramTile;
     const bool same = (a0 == b0);
     const int g = threadIdx.x >> 6, u = threadIdx.x & 63;
     const int ta = u & 7, tb = u >> 3;
     const uint32_t chunk = (rows + gridDim.x - 1) / gridDim.x;
     const uint32_t r0 = min(rows, blockIdx.x * chunk), r1 = min(rows, r0 + chunk);
+    const uint32_t nsteps = (r1 - r0 + kGramRows - 1) / kGramRows;
     float acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    // the next 64 rows are loaded into registers while the current ones are
-    // multiplied (all of a thread's loads in flight at once)
-    constexpr int PER = 64 * kGramTile / kLaThreads;
-    float na[PER], nb[PER];
-    auto fetch = [&](uint32_t base) {
-        const uint32_t nr = min(64u, r1 - base);
+    auto issue = [&](uint32_t st) {
+        const uint32_t base = r0 + st * kGramRows;
+        const uint32_t nr = min((uint32_t)kGramRows, r1 - base);
+        Stage& da = sa[st % kGramStages];
+        Stage& db = sb[st % kGramStages];
 #pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const int e = threadIdx.x + j * kLaThreads;
-            const int rr = e / kGramTile, cc = e % kGramTile;
-            float va = 0.f, vb = 0.f;
-            if (rr < (int)nr) {
-                const float* y = Y + (size_t)(base + rr) * Rp;
-                if (a0 + cc < R) va = __ldg(y + a0 + cc);
-                if (!same && b0 + cc < R) vb = __ldg(y + b0 + cc);
+        for (int k = 0; k < kGramRows * (kGramTile / 4) / kLaThreads; ++k) {
+            const int q = threadIdx.x + k * kLaThreads;
+            const int rr = q >> 3, c4 = q & 7;
+            const bool rowok = (uint32_t)rr < nr;
+            const float* row = Y + (size_t)(base + (rowok ? rr : 0)) * Rp;
+            const int ca = a0 + 4 * c4;
+            const bool oka = rowok && ca + 4 <= Rp;
+            cp_async16(&da[rr][4 * c4], oka ? row + ca : Y, oka ? 16 : 0);
+            if (!same) {
+                const int cb = b0 + 4 * c4;
+                const bool okb = rowok && cb + 4 <= Rp;
+                cp_async16(&db[rr][4 * c4], okb ? row + cb : Y, okb ? 16 : 0);
             }
-            na[j] = va;
-            nb[j] = vb;
         }
     };
-    if (r0 < r1) fetch(r0);
-    for (uint32_t base = r0; base < r1; base += 64) {
-        const uint32_t nr = min(64u, r1 - base);
 #pragma unroll
-        for (int j = 0; j < PER; ++j) {
-            const int e = threadIdx.x + j * kLaThreads;
-            const int rr = e / kGramTile, cc = e % kGramTile;
-            sa[rr][cc] = na[j];
-            if (!same) sb[rr][cc] = nb[j];
-        }
-        __syncthreads();
-        if (base + 64 < r1) fetch(base + 64);
-        const float (*tb_src)[kGramTile] = same ? sa : sb;
+    for (int st = 0; st < kGramStages - 1; ++st) {
+        if ((uint32_t)st < nsteps) issue(st);
+        cp_async_commit();
+    }
+    for (uint32_t st = 0; st < nsteps; ++st) {
+        cp_async_wait<kGramStages - 2>();
+        __syncthreads();           // step st landed for every thread; step st-1 consumed
+        if (st + kGramStages - 1 < nsteps) issue(st + kGramStages - 1);
+        cp_async_commit();
+        const uint32_t nr = min((uint32_t)kGramRows, r1 - (r0 + st * kGramRows));
+        const float (*A)[kGramTile] = sa[st % kGramStages];
+        const float (*B)[kGramTile] = same ? A : sb[st % kGramStages];
+#pragma unroll 4
         for (uint32_t rr = g; rr < nr; rr += 4) {
-            const float4 av = *reinterpret_cast<const float4*>(&sa[rr][4 * ta]);
-            const float4 bv = *reinterpret_cast<const float4*>(&tb_src[rr][4 * tb]);
+            const float4 av = *reinterpret_cast<const float4*>(&A[rr][4 * ta]);
+            const float4 bv = *reinterpret_cast<const float4*>(&B[rr][4 * tb]);
             const float x[4] = {av.x, av.y, av.z, av.w};
             const float y[4] = {bv.x, bv.y, bv.z, bv.w};
 #pragma unroll
@@ -398,8 +420,10 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(x[i], y[j], acc[i][j]);
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
+    __syncthreads();               // every stage consumed: reuse it for the row-group sums
+    float (*red)[kGramTile][kGramTile + 1] = reinterpret_cast<float (*)[kGramTile][kGramTile + 1]>(gsm);
     if (g > 0) {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -419,6 +443,22 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
                 if (a < R && b < R) partial[((size_t)blockIdx.x * R + a) * R + b] = v;
             }
     }
+}
+
+// Launches k_gram_partial (its shared memory is above the 48 KB default).
+int launch_gram_partial(dim3 grid, cudaStream_t st, const float* Y, uint32_t rows, int R, int Rp,
+                        double* partial) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    DGPU_CUDA(cudaGetDevice(&dev));
+    if (!attr_set[dev & 63]) {
+        DGPU_CUDA(cudaFuncSetAttribute(k_gram_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kGramSmem));
+        attr_set[dev & 63] = true;
+    }
+    k_gram_partial<<<grid, kLaThreads, kGramSmem, st>>>(Y, rows, R, Rp, partial);
+    DGPU_CUDA(cudaGetLastError());
+    return DGPU_OK;
 }
 
 // Sums the `chunks` partial Grams into partial[0 .. RR) (in place): a CTA
@@ -920,7 +960,7 @@ int gram_into(Plan& p, const LaLayout& L, int n, int normalise) {
     const int tiles = (p.R + kGramTile - 1) / kGramTile;
     const int chunks = (int)std::min<uint32_t>(kGramChunks, std::max<uint32_t>(1u, (p.dims[n] + 63) / 64));
     dim3 grid(chunks, tiles, tiles);
-    k_gram_partial<<<grid, kLaThreads, 0, p.stream>>>(p.Y[n], p.dims[n], p.R, p.Rp, L.partial);
+    DGPU_TRY(launch_gram_partial(grid, p.stream, p.Y[n], p.dims[n], p.R, p.Rp, L.partial));
     const size_t RR = (size_t)p.R * p.R;
     int fin_chunks = chunks;
     if (chunks > 8) {
@@ -1707,12 +1747,13 @@ extern "C" int dgpu_la_gram(void* stream, const float* Y, uint64_t rows, int R, 
     DGPU_CUDA(cudaMallocAsync((void**)&gd, RR * sizeof(double), st));
     DGPU_CUDA(cudaMallocAsync((void**)&lam, (size_t)R * sizeof(double), st));
     DGPU_CUDA(cudaMemsetAsync(G, 0, RR / R * Rp * sizeof(float), st));
-    k_gram_partial<<<dim3(chunks, tiles, tiles), kLaThreads, 0, st>>>(Y, (uint32_t)rows, R, Rp, part);
-    k_finalize_mode<<<1, 1024, 0, st>>>(part, chunks, R, Rp, 0, gd, G, nullptr, lam);
-    const cudaError_t e = cudaGetLastError();
+    const int rc = launch_gram_partial(dim3(chunks, tiles, tiles), st, Y, (uint32_t)rows, R, Rp, part);
+    if (rc == DGPU_OK) k_finalize_mode<<<1, 1024, 0, st>>>(part, chunks, R, Rp, 0, gd, G, nullptr, lam);
+    const cudaError_t e = rc == DGPU_OK ? cudaGetLastError() : cudaSuccess;
     cudaFreeAsync(part, st);
     cudaFreeAsync(gd, st);
     cudaFreeAsync(lam, st);
+    if (rc != DGPU_OK) return rc;
     if (e != cudaSuccess) {
         set_error("dgpu_la_gram: %s", cudaGetErrorString(e));
         return DGPU_ERR_CUDA;
