@@ -895,8 +895,21 @@ __global__ void k_loop_ctl(cudaGraphConditionalHandle h, const double* __restric
 __global__ void k_sumsq(const float* __restrict__ v, uint64_t n, double* __restrict__ out) {
     __shared__ double red[256];
     double s = 0;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
+    // float4 loads, four in flight per thread (v is 16-byte aligned: a slab
+    // column), then the scalar tail
+    const float4* v4 = reinterpret_cast<const float4*>(v);
+    const uint64_t n4 = n >> 2, stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += 4 * stride) {
+        float4 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            x[u] = q + u * stride < n4 ? __ldg(v4 + q + u * stride) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            s += (double)x[u].x * x[u].x + (double)x[u].y * x[u].y + (double)x[u].z * x[u].z +
+                 (double)x[u].w * x[u].w;
+    }
+    for (uint64_t i = 4 * n4 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const double x = v[i];
         s += x * x;
     }

@@ -19,8 +19,12 @@
  *      threads=T produces the same slab permutation as the reference built
  *      with --threads T.
  *
- *  Threading: a plan is not thread-safe; all of its device work is issued
- *  on one CUDA stream (its own, or one set with dgpu_plan_set_stream).
+ *  Threading: a plan is not thread-safe; its device work is ordered on one
+ *  CUDA stream (its own, or one set with dgpu_plan_set_stream).  Work that
+ *  the plan runs concurrently (the PingPong MTTKRP beside the remap, CP-ALS
+ *  solve maps, host-buffer transfers) goes to the plan's internal streams,
+ *  forked from and joined back into that stream before each call returns,
+ *  so the stream sees every call as complete work in order.
  * ========================================================================== */
 #ifndef DYNASOR_B200_H
 #define DYNASOR_B200_H
