@@ -81,15 +81,19 @@ constexpr int kRunWarps = kRunThreads / 32;
 // Nonzeros whose gathers a lane group keeps in flight together (U) and the
 // CTAs per SM the kernel is compiled for.  The kernel is bound by gather
 // latency, so occupancy (40-64 registers, 4-6 CTAs of 256 threads) pays more
-// than a deeper batch; BF16 rows take half the registers, so BF16 batches
-// deeper.
+// than a deeper batch, for BF16 rows as well.
 template <int N, int V, bool BF>
 struct RunBatch {
     static constexpr int kWork = (N - 1) * V;
     // measured on the 3-mode rank-32 Zipf tensor (MTTKRP ms per sweep):
-    // 4 CTAs/U=2 3.68, 5/1 3.60, 6/1 3.45, 8/1 3.66 (spills), 4/1 4.03
-    static constexpr int U = kWork <= 2 ? (BF ? 4 : 1) : (kWork <= 4 ? 2 : 1);
-    static constexpr int kMinBlocks = (kWork <= 2 && !BF) ? 6 : (N <= 4 ? 4 : 2);
+    //   FP32 4 CTAs/U=2 3.68, 5/1 3.60, 6/1 3.45, 8/1 3.66 (spills), 4/1 4.03;
+    //   BF16 4/4 3.65, 6/2 3.70, 6/1 3.08
+    // and on the 4-mode rank-64 tensor (NCopy CP-ALS iterations/s):
+    //   FP32 4/2 34.3, 3/2 32.8, 3/3 29.8, 5/1 36.0, 6/1 33.2 (spills);
+    //   BF16 4/2 31.2, 4/4 22.4, 3/3 28.8, 5/1 35.8, 6/1 36.9
+    static constexpr bool kQuad = (N == 4 && V == 1);
+    static constexpr int U = kWork <= 2 ? 1 : (kQuad ? 1 : (kWork <= 4 ? 2 : 1));
+    static constexpr int kMinBlocks = kWork <= 2 ? 6 : (kQuad ? (BF ? 6 : 5) : (N <= 4 ? 4 : 2));
 };
 
 // One CTA per tile.  Warp w owns the w-th contiguous slice of the tile and
