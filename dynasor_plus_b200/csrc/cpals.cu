@@ -27,6 +27,7 @@
 #include <functional>
 #include "dgpu_internal.h"
 #include "la_warp.cuh"
+#include "apply_map.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -182,7 +183,6 @@ k_apply_map(const float* __restrict__ Yhat, uint32_t rows, int R, int Rp,
 // loaded pair of entries feeds a multiply-add in every lane.  The next 8
 // rows are loaded while the current ones are multiplied.  Each output is the
 // same k-ordered fused multiply-add chain as in k_apply_map.
-constexpr int kMapRows = 8;                    // rows a warp stages at a time
 template <typename Real, int RP>
 __global__ void __launch_bounds__(kLaThreads, 2)
 k_apply_map_lanes(const float* __restrict__ Yhat, uint32_t rows, int R,
@@ -247,83 +247,6 @@ k_apply_map_lanes(const float* __restrict__ Yhat, uint32_t rows, int R,
             }
             const uint32_t i = b * kMapRows + r;
             if (i < rows) Y[(size_t)i * RP + c] = c < R ? (float)acc : 0.f;
-        }
-        __syncwarp();
-    }
-}
-
-// FP64 map on the FP64 tensor pipe (mma.sync m8n8k4 .f64) for Rp = RP in
-// {16, 32}: a warp multiplies blocks of 8 rows, Y(8 x RP) = Yhat(8 x RP) *
-// W(RP x RP), as RP/4 k-steps x RP/8 column tiles.  W's fragments stay in
-// registers (thread (g, t) = (lane / 4, lane % 4) holds W[4s + t][8j + g]);
-// the 8 rows are staged in a padded shared-memory slice (row stride RP + 4
-// floats: the A-fragment reads A[g][4s + t] fall in 32 distinct banks) and
-// converted to FP64 on the way into the fragments.  The next block is
-// loaded while the current one is multiplied.
-template <int RP>
-__global__ void __launch_bounds__(kLaThreads, 2)
-k_apply_map_dmma(const float* __restrict__ Yhat, uint32_t rows, int R,
-                 const double* __restrict__ W, float* __restrict__ Y)
-{
-    static_assert(RP == 16 || RP == 32, "two or four column tiles");
-    constexpr int NT = RP / 8, KS = RP / 4, LD = RP + 4;
-    constexpr int V4 = kMapRows * RP / 4 / 32;            // float4 loads per lane per block
-    __shared__ __align__(16) float hs[kLaThreads / 32][kMapRows][LD];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    double b[KS][NT];
-#pragma unroll
-    for (int ks = 0; ks < KS; ++ks)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-            const int k = 4 * ks + t, c = 8 * j + g;
-            b[ks][j] = (k < R && c < R) ? W[(size_t)k * R + c] : 0.0;
-        }
-    const uint32_t nblocks = (rows + kMapRows - 1) / kMapRows;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const float4* src = reinterpret_cast<const float4*>(Yhat);
-    const size_t n4 = (size_t)rows * RP / 4;
-    float4 pf[V4];
-    auto load = [&](uint32_t blk) {
-#pragma unroll
-        for (int v = 0; v < V4; ++v) {
-            const size_t q = (size_t)blk * (kMapRows * RP / 4) + v * 32 + lane;
-            pf[v] = q < n4 ? __ldg(src + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    };
-    uint32_t blk = gw;
-    if (blk < nblocks) load(blk);
-    for (; blk < nblocks; blk += nw) {
-#pragma unroll
-        for (int v = 0; v < V4; ++v) {
-            const int e = (v * 32 + lane) * 4;
-            *reinterpret_cast<float4*>(&hs[warp][e / RP][e % RP]) = pf[v];
-        }
-        __syncwarp();
-        if (blk + nw < nblocks) load(blk + nw);
-        double a[KS];
-#pragma unroll
-        for (int ks = 0; ks < KS; ++ks) a[ks] = (double)hs[warp][g][4 * ks + t];
-        double acc[NT][2];
-#pragma unroll
-        for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = 0.0;
-#pragma unroll
-        for (int ks = 0; ks < KS; ++ks)
-#pragma unroll
-            for (int j = 0; j < NT; ++j)
-                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                             : "+d"(acc[j][0]), "+d"(acc[j][1]) : "d"(a[ks]), "d"(b[ks][j]));
-        const uint32_t i = blk * kMapRows + g;
-        if (i < rows) {
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-                const int c = 8 * j + 2 * t;
-                float2 o;
-                o.x = c < R ? (float)acc[j][0] : 0.f;
-                o.y = c + 1 < R ? (float)acc[j][1] : 0.f;
-                *reinterpret_cast<float2*>(Y + (size_t)i * RP + c) = o;
-            }
         }
         __syncwarp();
     }
@@ -1069,9 +992,11 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
     if (p.Rp == 16 || p.Rp == 32) {
         const unsigned gm = grid_for((size_t)p.dims[n] * p.Rp / 4);
         if (solve_fp64 && p.Rp == 16)
-            k_apply_map_dmma<16><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.Wd, p.Y[n]);
+            k_apply_map_dmma<16><<<gm, kApplyThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, p.Rp,
+                                                                     L.Wd, 0, nullptr, p.Y[n]);
         else if (solve_fp64)
-            k_apply_map_dmma<32><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.Wd, p.Y[n]);
+            k_apply_map_dmma<32><<<gm, kApplyThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, p.Rp,
+                                                                     L.Wd, 0, nullptr, p.Y[n]);
         else if (p.Rp == 16)
             k_apply_map_lanes<float, 16><<<gm, kLaThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.R, L.W32, p.Y[n]);
         else

@@ -19,6 +19,7 @@
 // ============================================================================
 #include "dgpu_internal.h"
 #include "la_warp.cuh"
+#include "apply_map.cuh"
 
 #include <chrono>
 #include <cmath>
@@ -76,6 +77,92 @@ k_ms_gram_partial(const float* __restrict__ Y, uint32_t rows, int Rp, int Re,
     for (int q = 0; q < 16; ++q) {
         const int e = threadIdx.x + kMsThreads * q;
         if (e < RR) partial[((size_t)blockIdx.x * K + k) * RR + e] = acc[q];
+    }
+}
+
+__device__ __forceinline__ void ms_cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+                 :: "r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(src),
+                    "r"(src_bytes) : "memory");
+}
+
+// The same partial Gram blocks for RE in {16, 32} with register tiles: a
+// thread owns a 4 x 4 tile of its restart's RE x RE block (RE*RE/16
+// threads per row group, 256 / that many row groups taking interleaved
+// rows), rows stream in 64-row steps through a 4-stage cp.async ring, and
+// the row groups' tiles are added in group order at the end.
+template <int RE>
+__global__ void __launch_bounds__(kMsThreads)
+k_ms_gram_tiles(const float* __restrict__ Y, uint32_t rows, int Rp,
+                const int* __restrict__ active, float* __restrict__ partial)
+{
+    constexpr int TPG = RE * RE / 16;                 // threads per row group
+    constexpr int NG = kMsThreads / TPG;              // row groups
+    constexpr int ROWS = 64, STAGES = 4;
+    constexpr int CPR = RE / 4;                       // 16-byte chunks per row
+    static_assert(NG >= 1 && ROWS * CPR <= 2 * kMsThreads, "one or two copies per thread");
+    __shared__ __align__(16) float ring[STAGES][ROWS][RE];
+    const int k = blockIdx.y, K = gridDim.y;
+    if (active && !active[k]) return;
+    const int grp = threadIdx.x / TPG, u = threadIdx.x % TPG;
+    const int ta = u % (RE / 4), tb = u / (RE / 4);
+    const uint32_t chunk = (rows + gridDim.x - 1) / gridDim.x;
+    const uint32_t r0 = min(rows, blockIdx.x * chunk), r1 = min(rows, r0 + chunk);
+    const uint32_t nsteps = (r1 - r0 + ROWS - 1) / ROWS;
+    auto issue = [&](uint32_t st) {
+        const uint32_t base = r0 + st * ROWS;
+        const uint32_t nr = min((uint32_t)ROWS, r1 - base);
+        for (int q = threadIdx.x; q < ROWS * CPR; q += kMsThreads) {
+            const int rr = q / CPR, c4 = q % CPR;
+            const bool ok = (uint32_t)rr < nr;
+            const float* src = ok ? Y + (size_t)(base + rr) * Rp + (size_t)k * RE + 4 * c4 : Y;
+            ms_cp_async16(&ring[st % STAGES][rr][4 * c4], src, ok ? 16 : 0);
+        }
+    };
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+#pragma unroll
+    for (int st = 0; st < STAGES - 1; ++st) {
+        if ((uint32_t)st < nsteps) issue(st);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (uint32_t st = 0; st < nsteps; ++st) {
+        asm volatile("cp.async.wait_group %0;" :: "n"(STAGES - 2) : "memory");
+        __syncthreads();
+        if (st + STAGES - 1 < nsteps) issue(st + STAGES - 1);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        const uint32_t nr = min((uint32_t)ROWS, r1 - (r0 + st * ROWS));
+        const float (*A)[RE] = ring[st % STAGES];
+#pragma unroll 4
+        for (uint32_t rr = grp; rr < nr; rr += NG) {
+            const float4 av = *reinterpret_cast<const float4*>(&A[rr][4 * ta]);
+            const float4 bv = *reinterpret_cast<const float4*>(&A[rr][4 * tb]);
+            const float x[4] = {av.x, av.y, av.z, av.w};
+            const float y[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(x[i], y[j], acc[i][j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    // row-group tiles -> shared memory (the ring is free now), summed in
+    // group order by the first group
+    float* red = &ring[0][0][0];
+    static_assert(NG * RE * RE <= STAGES * ROWS * RE, "reduction fits in the ring");
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) red[(size_t)grp * RE * RE + (4 * ta + i) * RE + 4 * tb + j] = acc[i][j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < RE * RE; e += kMsThreads) {
+        double sum = 0.0;
+        for (int g = 0; g < NG; ++g) sum += (double)red[(size_t)g * RE * RE + e];
+        partial[((size_t)blockIdx.x * K + k) * RE * RE + e] = (float)sum;
     }
 }
 
@@ -159,6 +246,72 @@ k_ms_apply(const float* __restrict__ Yhat, uint32_t rows, int Rp, int K, int Re,
         if (j < Re) a0 += (Real)__ldg(yh + j) * (Real)__ldg(w + (size_t)j * Re);
         Y[i * Rp + col] = (float)(a0 + a1);
     }
+}
+
+// Column scaling by 1/lambda and (last mode) per-column <Y, Yhat> partials,
+// float4 per thread: every float4 a thread visits lies in one group of four
+// columns (the grid-stride is a multiple of Rp / 4), so the reciprocals and
+// the active flags are read once and the dot takes one shared-memory atomic
+// per column and thread.  Inactive restarts and padding columns are left as
+// they are (scale 1, no dot).
+__global__ void __launch_bounds__(kMsThreads)
+k_ms_scale4(float* __restrict__ Y, const float* __restrict__ Yhat, uint32_t rows, int Rp, int K,
+            int Re, const double* __restrict__ lam, const int* __restrict__ active,
+            double* __restrict__ dot_partial)
+{
+    extern __shared__ double sdot[];                         // [K*Re]
+    const int KR = K * Re;
+    if (Yhat) for (int c = threadIdx.x; c < KR; c += blockDim.x) sdot[c] = 0.0;
+    __syncthreads();
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t first = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int c0 = (int)(first % (size_t)(Rp >> 2)) * 4;
+    float inv[4];
+    bool use[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int col = c0 + j;
+        use[j] = col < KR && active[col / Re] != 0;
+        const double l = use[j] ? lam[col] : 0.0;
+        inv[j] = !use[j] ? 1.f : (l > 1e-20 ? (float)(1.0 / l) : 0.f);
+    }
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    float4* Y4 = reinterpret_cast<float4*>(Y);
+    const float4* H4 = reinterpret_cast<const float4*>(Yhat);
+    const size_t total4 = (size_t)rows * (Rp >> 2);
+    constexpr int U = 4;
+    for (size_t q = first; q < total4; q += U * stride) {
+        float4 y[U], h[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const size_t qq = q + u * stride;
+            y[u] = qq < total4 ? Y4[qq] : make_float4(0.f, 0.f, 0.f, 0.f);
+            h[u] = (Yhat && qq < total4) ? __ldg(H4 + qq) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const size_t qq = q + u * stride;
+            if (qq >= total4) break;
+            const float4 v = make_float4(y[u].x * inv[0], y[u].y * inv[1], y[u].z * inv[2],
+                                         y[u].w * inv[3]);
+            Y4[qq] = v;
+            if (Yhat) {
+                acc[0] += (double)v.x * (double)h[u].x;
+                acc[1] += (double)v.y * (double)h[u].y;
+                acc[2] += (double)v.z * (double)h[u].z;
+                acc[3] += (double)v.w * (double)h[u].w;
+            }
+        }
+    }
+    if (Yhat) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (use[j]) atomicAdd(&sdot[c0 + j], acc[j]);
+    }
+    __syncthreads();
+    if (Yhat)
+        for (int c = threadIdx.x; c < KR; c += blockDim.x)
+            dot_partial[(size_t)blockIdx.x * KR + c] = sdot[c];
 }
 
 // Column scaling by 1/lambda and (last mode) per-column <Y, Yhat> partials.
@@ -331,9 +484,16 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
     const int chunks_of = kMsChunks;
     auto gram = [&](int n, int normalise) -> int {
         const int chunks = (int)std::min<uint32_t>(chunks_of, std::max<uint32_t>(1u, (p.dims[n] + 63) / 64));
-        k_ms_gram_partial<<<dim3(chunks, K), kMsThreads, 0, p.stream>>>(p.Y[n], p.dims[n], p.Rp, Re,
-                                                                          normalise ? active : nullptr,
-                                                                          partial);
+        if (Re == 16)
+            k_ms_gram_tiles<16><<<dim3(chunks, K), kMsThreads, 0, p.stream>>>(
+                p.Y[n], p.dims[n], p.Rp, normalise ? active : nullptr, partial);
+        else if (Re == 32)
+            k_ms_gram_tiles<32><<<dim3(chunks, K), kMsThreads, 0, p.stream>>>(
+                p.Y[n], p.dims[n], p.Rp, normalise ? active : nullptr, partial);
+        else
+            k_ms_gram_partial<<<dim3(chunks, K), kMsThreads, 0, p.stream>>>(p.Y[n], p.dims[n], p.Rp, Re,
+                                                                              normalise ? active : nullptr,
+                                                                              partial);
         k_ms_finalize<<<K, kMsThreads, 0, p.stream>>>(partial, chunks, Re, normalise,
                                                       normalise ? active : nullptr,
                                                       Gd + (size_t)n * K * RR, lam, p.lambda);
@@ -364,7 +524,17 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
         else
             k_ms_solve<float><<<K, 32, solve_sm, p.stream>>>(Gd, N, n, Re, o.ridge, active, W);
         const unsigned g = ms_grid((size_t)p.dims[n] * KR);
-        if (o.solve_fp64)
+        if (o.solve_fp64 && (Re == 16 || Re == 32)) {
+            // block-diagonal map, one column block per restart, on the FP64
+            // tensor pipe
+            const unsigned gx = std::max(1u, std::min(g, (unsigned)(148 * 2 * 8 / K + 1)));
+            if (Re == 16)
+                k_apply_map_dmma<16><<<dim3(gx, K), kApplyThreads, 0, p.stream>>>(
+                    p.Yhat[n], p.dims[n], Re, p.Rp, W, (size_t)RR, active, p.Y[n]);
+            else
+                k_apply_map_dmma<32><<<dim3(gx, K), kApplyThreads, 0, p.stream>>>(
+                    p.Yhat[n], p.dims[n], Re, p.Rp, W, (size_t)RR, active, p.Y[n]);
+        } else if (o.solve_fp64)
             k_ms_apply<double><<<g, kMsThreads, 0, p.stream>>>(p.Yhat[n], p.dims[n], p.Rp, K, Re, W,
                                                                active, p.Y[n]);
         else
@@ -373,8 +543,12 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
         DGPU_CUDA(cudaGetLastError());
         DGPU_TRY(gram(n, 1));
         const unsigned gs = std::min<unsigned>(ms_grid((size_t)p.dims[n] * KR), kMsChunks);
-        k_ms_scale<<<gs, kMsThreads, (size_t)KR * sizeof(double), p.stream>>>(
-            p.Y[n], last ? p.Yhat[n] : nullptr, p.dims[n], p.Rp, K, Re, lam, active, dot);
+        if (((size_t)gs * kMsThreads) % (size_t)(p.Rp / 4) == 0)
+            k_ms_scale4<<<gs, kMsThreads, (size_t)KR * sizeof(double), p.stream>>>(
+                p.Y[n], last ? p.Yhat[n] : nullptr, p.dims[n], p.Rp, K, Re, lam, active, dot);
+        else
+            k_ms_scale<<<gs, kMsThreads, (size_t)KR * sizeof(double), p.stream>>>(
+                p.Y[n], last ? p.Yhat[n] : nullptr, p.dims[n], p.Rp, K, Re, lam, active, dot);
         DGPU_CUDA(cudaGetLastError());
         p.yb_stale[n] = true;
         return DGPU_OK;

@@ -10,15 +10,18 @@ from conftest import load_golden, rel_fro
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("Re", [8, 16])
 @pytest.mark.parametrize("layout,kernel,graphs", [("pingpong", "gs", True), ("ncopy", "gs", True),
                                                   ("pingpong", "gs", False),
                                                   ("ncopy", "jacobi", True)])
-def test_restarts_follow_independent_runs(layout, kernel, graphs):
+def test_restarts_follow_independent_runs(layout, kernel, graphs, Re):
+    """Re = 16 takes the block-diagonal map on the FP64 tensor pipe, Re = 8
+    the scalar one."""
     import dynasor_plus_b200 as d
     g = load_golden("ref_cpals_r5.npz")
     dims = g["dims"]
     idx = [g[f"idx{n}"] for n in range(len(dims))]
-    K, Re = 4, 8
+    K = 4
     iters = 3 if kernel == "jacobi" else 30
     tol = 0.0 if kernel == "jacobi" else 1e-4
     p = d.Plan(dims, g["vals"], idx, threads=int(g["T"]), rank=K * Re, layout=layout)
