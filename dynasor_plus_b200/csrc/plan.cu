@@ -162,6 +162,11 @@ int timing_collect(Plan& p) {
 Plan::~Plan() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    // internal streams are joined into `stream` before every call returns;
+    // after a failed call some of their work may not be, so wait for them
+    // before freeing anything they may still read
+    for (cudaStream_t s2 : {copy_stream, side_stream, ovl_stream})
+        if (s2) cudaStreamSynchronize(s2);
     for (auto& t : pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     for (auto e : event_pool) cudaEventDestroy(e);
     for (auto& s : slab) dev_free(s.raw);
