@@ -23,8 +23,8 @@ import os
 
 import numpy as np
 
-from ._lib import (CpOptions, CpResult, Coo, DgpuError, DnpInfo, PlanInfo, PlanOpts, TensorDesc, check,
-                   lib, LIB_PATH)
+from ._lib import (ComputePlan, ComputePlanInput, CpOptions, CpResult, Coo, DgpuError, DnpInfo,
+                   PlanInfo, PlanOpts, TensorDesc, check, lib, LIB_PATH)
 
 __all__ = ["Plan", "DgpuError", "cpals_batch", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
            "dnp_peek",
@@ -38,6 +38,66 @@ LAYOUTS = {"pingpong": PINGPONG, "ncopy": NCOPY, "morton": MORTON, "auto": AUTO}
 LAYOUT_NAMES = {PINGPONG: "pingpong", NCOPY: "ncopy", MORTON: "morton"}
 PRECISIONS = {"fp32": 0, "bf16": 1}
 ACCUMS = {"auto": 0, "rowrun": 1, "private": 2}
+
+
+def _kernel_code(kernel) -> int:
+    """CP-ALS kernel keyword -> DGPU_CP_* (the reference's --cp-kernel words)."""
+    k = str(kernel).lower()
+    if k in ("jacobi", "all-modes", "all_modes", "js"):
+        return 1
+    if k == "auto":
+        return 2
+    return 0
+
+
+_IMPL = {0: "Element", 1: "Fiber", 2: "FiberCSR"}
+_ACCUM = {0: "all-modes", 1: "rowrun", 2: "private"}
+_LAYOUT = {0: "pingpong", 1: "ncopy", 4: "morton"}
+
+
+def _compute_plan_dict(cp, N) -> dict:
+    return {"layout": _LAYOUT.get(cp.layout, cp.layout),
+            "kernel": "jacobi" if cp.kernel == 1 else "gs",
+            "kernel_reason": cp.kernel_reason.decode(), "kernel_source": cp.kernel_source.decode(),
+            "per_mode": [_IMPL[cp.per_mode[n]] for n in range(N)],
+            "accum": [_ACCUM.get(cp.accum[n], cp.accum[n]) for n in range(N)],
+            "rank_tile": list(cp.rank_tile[:N]),
+            "precision": "bf16" if cp.precision == 1 else "fp32",
+            "rank_padded": cp.rank_padded, "threads": cp.threads,
+            "ofibs_bytes": int(cp.ofibs_bytes), "factor_bytes": int(cp.factor_bytes),
+            "budget_bytes": int(cp.budget_bytes), "device_bytes": int(cp.device_bytes),
+            "_raw": cp}
+
+
+def compute_plan_decide(dims, nnz, rank, threads, layout="pingpong", fiber=True,
+                        kernel_class=None, avg_fiber_len=None, host_avail_bytes=0,
+                        kernel="auto") -> dict:
+    """The compute plan's decisions from tensor facts alone (host only, no
+    device): dyn_build_compute_plan's kernel rule and per-mode class
+    (src/dynasor_preprocess.cpp:1179-1363)."""
+    N = len(dims)
+    inp = ComputePlanInput()
+    inp.num_modes = N
+    inp.nnz = int(nnz)
+    for n in range(min(N, len(inp.mode_size))):    # more modes: rejected by the library
+        inp.mode_size[n] = int(dims[n])
+        inp.kernel_class[n] = int(kernel_class[n]) if kernel_class is not None else 0
+        inp.avg_fiber_len[n] = float(avg_fiber_len[n]) if avg_fiber_len is not None else 0.0
+    inp.rank_padded = padded_rank(rank)
+    inp.threads = int(threads)
+    inp.layout = {"pingpong": 0, "ncopy": 1, "morton": 4}[layout]
+    inp.fiber = 1 if fiber else 0
+    inp.host_avail_bytes = int(host_avail_bytes)
+    cp = ComputePlan()
+    check(lib().dgpu_compute_plan_decide(C.byref(inp), str(kernel).encode(), C.byref(cp)))
+    return _compute_plan_dict(cp, N)
+
+
+def format_compute_plan(plan_dict, prefix="[plan]") -> str:
+    """The plan banner (dyn_print_compute_plan's rows)."""
+    buf = C.create_string_buffer(2048)
+    check(lib().dgpu_format_compute_plan(C.byref(plan_dict["_raw"]), prefix.encode(), buf, 2048))
+    return buf.value.decode()
 
 
 def padded_rank(R: int) -> int:
@@ -303,7 +363,7 @@ class Plan:
         o.tol = float(tol)
         o.seed = int(seed)
         o.ridge = float(ridge)
-        o.kernel = 1 if kernel in ("jacobi", "all-modes", "all_modes", "js") else 0
+        o.kernel = _kernel_code(kernel)
         o.solve_fp64 = 1 if solve_fp64 else 0
         o.use_init = 1 if use_init else 0
         o.verbose = 1 if verbose else 0
@@ -330,7 +390,7 @@ class Plan:
         o.tol = float(tol)
         o.seed = int(seed)
         o.ridge = float(ridge)
-        o.kernel = 1 if kernel in ("jacobi", "all-modes", "all_modes", "js") else 0
+        o.kernel = _kernel_code(kernel)
         o.solve_fp64 = 1 if solve_fp64 else 0
         o.use_init = 1 if use_init else 0
         o.verbose = 1 if verbose else 0
@@ -347,6 +407,14 @@ class Plan:
                  "total_time_s": r.total_time_s,
                  "fit_history": hist[k, :r.iters_done].copy(),
                  "lambda": lam[k * Re:(k + 1) * Re].copy()} for k, r in enumerate(res)]
+
+    def compute_plan(self, kernel="auto") -> dict:
+        """dyn_build_compute_plan for this plan: the CP-ALS kernel the
+        reference's rule picks, the per-mode kernel class, and what this
+        engine runs per mode (accumulation scheme, rank tile)."""
+        cp = ComputePlan()
+        check(lib().dgpu_build_compute_plan(self._h, str(kernel).encode(), C.byref(cp)))
+        return _compute_plan_dict(cp, self.N)
 
     def tensor_norm_sq(self) -> float:
         out = C.c_double(0)
@@ -453,7 +521,7 @@ def cpals_batch(plans, max_iters=50, tol=1e-4, seed=42, ridge=1e-10, kernel="gs"
     o.tol = float(tol)
     o.seed = int(seed)
     o.ridge = float(ridge)
-    o.kernel = 1 if kernel in ("jacobi", "all-modes", "all_modes", "js") else 0
+    o.kernel = _kernel_code(kernel)
     o.solve_fp64 = 1 if solve_fp64 else 0
     o.use_init = 1 if use_init else 0
     o.graphs = 1 if graphs else 0

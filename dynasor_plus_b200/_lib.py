@@ -64,6 +64,22 @@ class CpResult(C.Structure):
                 ("mttkrp_time_s", C.c_double), ("linalg_time_s", C.c_double)]
 
 
+class ComputePlanInput(C.Structure):
+    _fields_ = [("num_modes", C.c_int), ("nnz", C.c_uint64), ("mode_size", C.c_uint32 * MAX_MODES),
+                ("rank_padded", C.c_int), ("threads", C.c_int), ("layout", C.c_int),
+                ("fiber", C.c_int), ("kernel_class", C.c_int * MAX_MODES),
+                ("avg_fiber_len", C.c_double * MAX_MODES), ("host_avail_bytes", C.c_uint64)]
+
+
+class ComputePlan(C.Structure):
+    _fields_ = [("layout", C.c_int), ("kernel", C.c_int), ("kernel_reason", C.c_char * 48),
+                ("kernel_source", C.c_char * 16), ("per_mode", C.c_int * MAX_MODES),
+                ("accum", C.c_int * MAX_MODES), ("rank_tile", C.c_int * MAX_MODES),
+                ("precision", C.c_int), ("num_modes", C.c_int), ("rank_padded", C.c_int),
+                ("threads", C.c_int), ("ofibs_bytes", C.c_uint64), ("factor_bytes", C.c_uint64),
+                ("budget_bytes", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
 class KernelTiming(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("launches", C.c_uint64), ("total_ms", C.c_double),
                 ("bytes", C.c_double)]
@@ -112,6 +128,11 @@ _SIGS = {
                                         C.c_void_p]),
     "dgpu_cpals_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CpOptions), C.c_void_p,
                                    C.c_void_p]),
+    "dgpu_compute_plan_decide": (C.c_int, [C.POINTER(ComputePlanInput), C.c_char_p,
+                                           C.POINTER(ComputePlan)]),
+    "dgpu_build_compute_plan": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(ComputePlan)]),
+    "dgpu_format_compute_plan": (C.c_int, [C.POINTER(ComputePlan), C.c_char_p, C.c_char_p,
+                                           C.c_size_t]),
     "dgpu_la_gram": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_void_p]),
     "dgpu_tensor_norm_sq": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "dgpu_model_values": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -514,13 +514,55 @@ void dgpu_cp_options_default(dgpu_cp_options* o) {
     o->graphs = 1;
 }
 
+namespace {
+// BF16-gather CP-ALS gathers the last mode's rows in FP32: the last mode's
+// Yhat gives the fit's <X, M> = sum_r lambda_r <Y[N-1][:, r], Yhat[N-1][:, r]>
+// (src/dynasor_linalg.cpp:324-366), and a Yhat computed from BF16-rounded
+// factors moves that term, and with it the fit, by up to ~2e-4 on small
+// well-fitted tensors (FP64 CP-ALS with BF16-rounded gathers on a 20 x 25 x
+// 30 rank-5 tensor; ~6e-6 with the last mode in FP32).  Set for the length
+// of one run, reset on every exit path.
+// DGPU_CP_AUTO: the compute plan's kernel (the reference's pick_auto rule,
+// src/dynasor_preprocess.cpp:1252-1285); with verbose the plan banner is
+// printed first, as the reference's driver prints dyn_print_compute_plan.
+int resolve_kernel(Plan& p, dgpu_cp_options& o) {
+    if (o.kernel != DGPU_CP_GAUSS_SEIDEL && o.kernel != DGPU_CP_JACOBI && o.kernel != DGPU_CP_AUTO) {
+        set_error("cpals: unknown kernel %d", o.kernel);
+        return DGPU_ERR_ARG;
+    }
+    if (o.kernel != DGPU_CP_AUTO) return DGPU_OK;
+    dgpu_compute_plan cp;
+    DGPU_TRY(dgpu_build_compute_plan(reinterpret_cast<dgpu_plan*>(&p), nullptr, &cp));
+    o.kernel = cp.kernel;
+    if (o.verbose) {
+        char banner[1024];
+        if (dgpu_format_compute_plan(&cp, "[plan]", banner, sizeof(banner)) == DGPU_OK)
+            std::fputs(banner, stdout);
+    }
+    return DGPU_OK;
+}
+
+struct LastModeFp32 {
+    std::vector<Plan*> ps;
+    LastModeFp32(Plan* const* p, int count) : ps(p, p + count) {
+        for (Plan* q : ps) q->fp32_gather_mode = q->N - 1;
+    }
+    ~LastModeFp32() {
+        for (Plan* q : ps) q->fp32_gather_mode = -1;
+    }
+};
+}  // namespace
+
 int dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt, dgpu_cp_result* res,
                double* fit_history) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     API_GUARD(p);
     if (!opt || !res) { set_error("dgpu_cpals: null argument"); return DGPU_ERR_ARG; }
     if (opt->max_iters < 0) { set_error("dgpu_cpals: max_iters < 0"); return DGPU_ERR_ARG; }
-    return cpals_run(*p, *opt, *res, fit_history);
+    dgpu_cp_options o = *opt;
+    DGPU_TRY(resolve_kernel(*p, o));
+    LastModeFp32 fp32_last(&p, 1);
+    return cpals_run(*p, o, *res, fit_history);
 }
 
 int dgpu_cpals_batch(dgpu_plan* const* plans, int count, const dgpu_cp_options* opt,
@@ -544,7 +586,26 @@ int dgpu_cpals_batch(dgpu_plan* const* plans, int count, const dgpu_cp_options* 
     }
     Plan* p = ps[0];
     API_GUARD(p);
-    return cpals_batch_run(ps.data(), count, *opt, res, fit_history);
+    // one kernel for the batch: DGPU_CP_AUTO must resolve alike on every plan
+    dgpu_cp_options o = *opt;
+    if (o.kernel == DGPU_CP_AUTO) {
+        int kind = -1;
+        for (int k = 0; k < count; ++k) {
+            dgpu_cp_options ok = o;
+            ok.verbose = 0;
+            DGPU_TRY(resolve_kernel(*ps[k], ok));
+            if (kind >= 0 && ok.kernel != kind) {
+                set_error("dgpu_cpals_batch: the plans' compute plans choose different kernels; "
+                          "pass DGPU_CP_GAUSS_SEIDEL or DGPU_CP_JACOBI");
+                return DGPU_ERR_ARG;
+            }
+            kind = ok.kernel;
+        }
+        o.kernel = kind;
+    }
+    DGPU_TRY(resolve_kernel(*p, o));
+    LastModeFp32 fp32_last(ps.data(), count);
+    return cpals_batch_run(ps.data(), count, o, res, fit_history);
 }
 
 int dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* opt,
@@ -566,7 +627,10 @@ int dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options* 
         set_error("dgpu_cpals_multistart: rank per restart %d exceeds 64", p->R / restarts);
         return DGPU_ERR_ARG;
     }
-    return cpals_multistart_run(*p, restarts, *opt, res, fit_history);
+    dgpu_cp_options o = *opt;
+    DGPU_TRY(resolve_kernel(*p, o));
+    LastModeFp32 fp32_last(&p, 1);
+    return cpals_multistart_run(*p, restarts, o, res, fit_history);
 }
 
 }  // extern "C"

@@ -200,6 +200,11 @@ struct Plan {
     float*       Yhat[kMaxModes] = {nullptr};
     __nv_bfloat16* Yb[kMaxModes] = {nullptr};
     bool         yb_stale[kMaxModes] = {};
+    // Under BF16 precision, the mode whose MTTKRP still gathers FP32 rows
+    // (-1: none).  CP-ALS sets it to the last mode for the length of a run:
+    // that mode's Yhat gives the fit's <X, M> term, and BF16-rounded gathers
+    // there move the fit by up to ~2e-4 on small, well-fitted tensors.
+    int          fp32_gather_mode = -1;
     uint32_t*    part_cnt = nullptr;            // [chunks x buckets] counts
     uint32_t*    part_off = nullptr;            // [chunks x buckets] in-segment prefixes
     size_t       part_cap = 0;                  // entries of each

@@ -159,6 +159,25 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     uint32_t cur = 0xffffffffu;
     bool first_run = true;                 // the run at the start of this group's slice
 
+    // U == 1: the gathered rows stay in registers from one nonzero to the
+    // next, and a row is loaded only when its index differs from the
+    // previous nonzero's.  Inside a fiber-sorted row run of mode n the
+    // nonzeros keep the previous mode's processing order, which is sorted by
+    // that mode's index, so equal (i_n, i_{n-1}) pairs are consecutive: on
+    // the 3-mode Zipf(1.1) tensor 56-68% of one of the two gathers repeat
+    // the previous nonzero's row.  The arithmetic is unchanged (same values,
+    // same order); only the load is skipped.
+    float yk[N][V][4];
+    uint32_t last[N];
+#pragma unroll
+    for (int w = 0; w < N; ++w) {
+        last[w] = 0xffffffffu;
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) yk[w][v][q] = 0.f;
+    }
+
     // prefetch registers for one chunk
     uint32_t pf[LPE][SW];
     auto prefetch = [&](uint32_t ch) {
@@ -208,13 +227,32 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
 #pragma unroll
                 for (int w = 0; w < N; ++w) {
                     const uint32_t id = s[1 + w];
+                    if constexpr (U == 1) {
+                        if (w != n && id != last[w]) {
+                            last[w] = id;
 #pragma unroll
-                    for (int v = 0; v < V; ++v) {
-                        const int c4 = gl + v * G;
-                        float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
-                        y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
-                        y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
+                            for (int v = 0; v < V; ++v) {
+                                const int c4 = gl + v * G;
+                                if (V == 1 || c4 < C4) {
+                                    const float4 g4 = gather4<BF>(F, w, id, ld, c4);
+                                    yk[w][v][0] = g4.x; yk[w][v][1] = g4.y;
+                                    yk[w][v][2] = g4.z; yk[w][v][3] = g4.w;
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int v = 0; v < V; ++v)
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) y[u][w][v][q] = yk[w][v][q];
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < V; ++v) {
+                            const int c4 = gl + v * G;
+                            float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
+                            y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
+                            y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
+                        }
                     }
                 }
             }
@@ -608,7 +646,7 @@ int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
         if (w != n && w != w0) { wl = w; break; }
     FacPtrs F{};
     for (int w = 0; w < p.N; ++w) { F.Y[w] = p.Y[w]; F.Yb[w] = p.Yb[w]; }
-    const bool bf = (p.precision == DGPU_PREC_BF16);
+    const bool bf = (p.precision == DGPU_PREC_BF16) && n != p.fp32_gather_mode;
     if (bf)
         for (int w = 0; w < p.N; ++w)
             if (w != n && p.yb_stale[w]) DGPU_TRY(launch_to_bf16(p, w));

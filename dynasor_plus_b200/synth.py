@@ -9,6 +9,9 @@ float32[nnz], ``idx`` a list of N uint32[nnz] arrays with 0-based indices.
 * ``cp_truth``      3-mode rank-5 CP model with U(0,1) factors at distinct
                     uniform coordinates plus N(0, (1% mean)^2) noise
                     (the 200^3 / 100k-nonzero CP-ALS workload).
+* ``tensor_batch``  many small 3-mode CP-model tensors of uneven size: dims
+                    log-uniform per mode, nnz log-uniform (the 32-tensor
+                    batch workload: [1e3, 1e5] per mode, [1e4, 5e6] nnz).
 * ``zipf``          per-mode Zipf(s) coordinates over a seed-permuted index
                     set, duplicates merged, LogNormal(0,1) values (the
                     1,000,000 x 200,000 x 50,000 MTTKRP workload when called
@@ -63,6 +66,23 @@ def cp_truth(dims=(200, 200, 200), nnz=100_000, rank=5, noise=0.01, seed=1, fact
     v = v + rng.normal(0.0, noise * v.mean(), nnz)
     idx = [np.ascontiguousarray(coords[:, n], np.uint32) for n in range(len(dims))]
     return dims, v.astype(np.float32), idx
+
+
+def tensor_batch(count=32, seed=17, dim_range=(1_000, 100_000), nnz_range=(10_000, 5_000_000),
+                 rank=4, noise=0.01):
+    """`count` independent ``cp_truth`` tensors (rank-`rank` U(0,1) truth plus
+    `noise` relative Gaussian noise), each with three mode sizes drawn
+    log-uniform in `dim_range` and a nonzero count drawn log-uniform in
+    `nnz_range`.  Returns a list of (dims, vals, idx)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(dim_range[0]), np.log(dim_range[1])
+    nlo, nhi = np.log(nnz_range[0]), np.log(nnz_range[1])
+    out = []
+    for k in range(count):
+        dims = tuple(int(x) for x in np.exp(rng.uniform(lo, hi, 3)))
+        nnz = int(np.exp(rng.uniform(nlo, nhi)))
+        out.append(cp_truth(dims, nnz, rank, noise, seed=int(rng.integers(0, 2**31))))
+    return out
 
 
 def _zipf_cdf(I, s):

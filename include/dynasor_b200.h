@@ -67,6 +67,8 @@ extern "C" {
 
 #define DGPU_CP_GAUSS_SEIDEL 0   /* CpKernel::GaussSeidel                 */
 #define DGPU_CP_JACOBI       1   /* CpKernel::Jacobi (all-modes pass)     */
+#define DGPU_CP_AUTO         2   /* the compute plan's choice (the
+                                    reference's --cp-kernel auto)        */
 
 #define DGPU_PREC_FP32       0   /* FP32 gathers, FP32 accumulation       */
 #define DGPU_PREC_BF16       1   /* BF16 gathers (FP32 master factors)    */
@@ -133,7 +135,8 @@ typedef struct {
     double    tol;                /* stop when |fit_i - fit_{i-1}| < tol  */
     uint64_t  seed;               /* N(0,1) init seed (default 42)        */
     double    ridge;              /* relative ridge (default 1e-10)       */
-    int       kernel;             /* DGPU_CP_*                            */
+    int       kernel;             /* DGPU_CP_* (DGPU_CP_AUTO: the compute
+                                     plan's rule; default Gauss-Seidel)  */
     int       solve_fp64;         /* 1: FP64 Cholesky + solve (default)   */
     int       use_init;           /* 1: start from the uploaded factors   */
     int       verbose;            /* print the reference's [cpals] lines  */
@@ -306,6 +309,68 @@ int  dgpu_cpals_multistart(dgpu_plan* plan, int restarts, const dgpu_cp_options*
  * count x max_iters fits, row k for plans[k]. */
 int  dgpu_cpals_batch(dgpu_plan* const* plans, int count, const dgpu_cp_options* opt,
                       dgpu_cp_result* res, double* fit_history);
+
+/* ---- compute plan (replaces ComputePlan, dyn_build_compute_plan and
+ *      dyn_print_compute_plan: include/dynasor_common.h:244-320,
+ *      src/dynasor_preprocess.cpp:1179-1399) ---------------------------------
+ * The run-time decisions of a plan in one record: the CP-ALS kernel
+ * (Jacobi or Gauss-Seidel, chosen by the reference's rule: Morton layout ->
+ * Jacobi; nnz < 1M -> Gauss-Seidel; N == 3 and Rp >= 64, or Rp >= 128 ->
+ * Gauss-Seidel; the reference's per-thread all-modes output copies
+ * (threads x sum_n I_n*Rp*4, each rounded to 64 B) >= min(MemAvailable/4,
+ * 8 GiB) -> Gauss-Seidel; else Jacobi), the reference's per-mode kernel
+ * class, and what this engine runs per mode (accumulation scheme, rank
+ * tile).  kernel_cli takes the reference's keywords ("auto", "jacobi",
+ * "all-modes", "js", "gs", "gauss-seidel", "per-mode", ...; NULL = auto);
+ * the DYN_CP_KERNEL environment variable overrides it as in the reference. */
+#define DGPU_IMPL_ELEMENT    0   /* KernelImpl::Element                   */
+#define DGPU_IMPL_FIBER      1   /* KernelImpl::Fiber                     */
+#define DGPU_IMPL_FIBERCSR   2   /* KernelImpl::FiberCSR                  */
+
+/* Tensor facts the decision needs (no device involved). */
+typedef struct {
+    int       num_modes;
+    uint64_t  nnz;
+    uint32_t  mode_size[DGPU_MAX_MODES];
+    int       rank_padded;
+    int       threads;
+    int       layout;                           /* DGPU_LAYOUT_PINGPONG/NCOPY/MORTON */
+    int       fiber;                            /* NCopy copies fiber-sorted  */
+    int       kernel_class[DGPU_MAX_MODES];     /* 0 sparse, 1 medium, 2 dense */
+    double    avg_fiber_len[DGPU_MAX_MODES];
+    uint64_t  host_avail_bytes;                 /* 0: MemAvailable of /proc/meminfo */
+} dgpu_compute_plan_input;
+
+typedef struct {
+    int       layout;                           /* DGPU_LAYOUT_* of the plan  */
+    int       kernel;                           /* DGPU_CP_GAUSS_SEIDEL / JACOBI */
+    char      kernel_reason[48];
+    char      kernel_source[16];                /* auto | cli-kernel | env-kernel */
+    int       per_mode[DGPU_MAX_MODES];         /* DGPU_IMPL_* (reference class) */
+    int       accum[DGPU_MAX_MODES];            /* DGPU_ACCUM_ROWRUN / PRIVATE used
+                                                   here (0: all-modes pass only) */
+    int       rank_tile[DGPU_MAX_MODES];        /* columns per slab pass
+                                                   (0: tuned at first use) */
+    int       precision;                        /* DGPU_PREC_*                */
+    int       num_modes;
+    int       rank_padded;
+    int       threads;
+    uint64_t  ofibs_bytes;                      /* reference all-modes copies  */
+    uint64_t  factor_bytes;                     /* sum_n I_n * Rp * 4 * 2      */
+    uint64_t  budget_bytes;                     /* min(MemAvailable/4, 8 GiB)  */
+    uint64_t  device_bytes;                     /* HBM held by the plan        */
+} dgpu_compute_plan;
+
+/* The decision from tensor facts alone (host only; device fields zero). */
+int dgpu_compute_plan_decide(const dgpu_compute_plan_input* in, const char* kernel_cli,
+                             dgpu_compute_plan* out);
+/* The decision for a built plan, with its device facts filled in. */
+int dgpu_build_compute_plan(const dgpu_plan* plan, const char* kernel_cli,
+                            dgpu_compute_plan* out);
+/* The plan banner (one "<prefix> key : value" line per row, like
+ * dyn_print_compute_plan) into buf; DGPU_ERR_ARG when cap is too small. */
+int dgpu_format_compute_plan(const dgpu_compute_plan* cp, const char* prefix, char* buf,
+                             size_t cap);
 
 /* ---- small dense kernels (replace la::*, include/dynasor_linalg.h:33-127),
  *      device pointers, FP32 row-major with leading dimension Rp --------- */

@@ -242,10 +242,13 @@ def uniform_factors(seed, dims, R):
     return Y
 
 
-def cpals_f64(dims, vals, idx, R, max_iters, tol, seed=42, ridge=1e-10, Y0=None, jacobi=False):
+def cpals_f64(dims, vals, idx, R, max_iters, tol, seed=42, ridge=1e-10, Y0=None, jacobi=False,
+              bf16_gathers=False, last_mode_fp32=False):
     """FP64 CP-ALS (Gauss-Seidel, or Jacobi: all MTTKRPs from the iteration's
     starting factors) from the reference's seed-`seed` N(0,1) init (or from
-    Y0).  Returns (fit_history, Y, lambda)."""
+    Y0).  bf16_gathers: the MTTKRP reads factors rounded to BF16 (the
+    arithmetic of the BF16-gather path, otherwise FP64).  Returns
+    (fit_history, Y, lambda)."""
     L = _oracle_lib()
     N = len(dims)
     Rp = padded_rank(R)
@@ -258,7 +261,9 @@ def cpals_f64(dims, vals, idx, R, max_iters, tol, seed=42, ridge=1e-10, Y0=None,
     idx = [np.ascontiguousarray(i, np.uint32) for i in idx]
     it = L.orc_cpals_f64(N, len(vals), np.ascontiguousarray(dims, np.uint32),
                          np.ascontiguousarray(vals, np.float32), _ptr_array(idx), R, Rp,
-                         max_iters, tol, ridge, _ptr_array(Y), fit, lam, 1 if jacobi else 0)
+                         max_iters, tol, ridge, _ptr_array(Y), fit, lam,
+                         (1 if jacobi else 0) | (2 if bf16_gathers else 0)
+                         | (4 if last_mode_fp32 else 0))
     return fit[:it], Y, lam
 
 
@@ -309,6 +314,9 @@ def _ref_lib():
         L.ref_build_morton.argtypes = [C.c_void_p]
         L.ref_morton_get.restype = C.c_int
         L.ref_morton_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_compute_plan.restype = C.c_int
+        L.ref_compute_plan.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
+                                       C.c_char_p, C.c_int, _i32p]
         L.ref_all_modes_morton.restype = C.c_double
         L.ref_all_modes_morton.argtypes = [C.c_void_p]
         _rlib = L
@@ -369,6 +377,15 @@ class Reference:
                                    vals.ctypes.data)
         assert rc == 0
         return mask, bits, keys, vals
+
+    def compute_plan(self, rank_padded, layout="pingpong", kernel_cli="auto"):
+        """dyn_build_compute_plan on the built tensor: (kernel 0 GS / 1
+        Jacobi, reason, per-mode kernel class list)."""
+        reason = C.create_string_buffer(64)
+        per = np.zeros(self.N, np.int32)
+        k = self.L.ref_compute_plan(self.h, int(rank_padded), int(self.T), layout.encode(),
+                                    kernel_cli.encode(), reason, 64, per)
+        return k, reason.value.decode(), [int(x) for x in per]
 
     def all_modes_morton(self):
         return self.L.ref_all_modes_morton(self.h)

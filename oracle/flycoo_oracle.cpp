@@ -1,7 +1,9 @@
 // ============================================================================
 //  flycoo_oracle.cpp -- TEST INFRASTRUCTURE ONLY (the oracle).
 //
-//  A plain, single-threaded CPU restatement of the Dynasor+ hot path, used
+//  A plain CPU restatement of the Dynasor+ hot path (single-threaded except
+//  the FP64 CP-ALS, whose per-row sums and Gram blocks run under OpenMP in
+//  an order that does not depend on the thread count), used
 //  only as a checker by tests/, __graft_entry__.smoke() and the CPU-baseline
 //  leg of bench.py.  The product library never links or calls it.
 //
@@ -337,18 +339,36 @@ void orc_mttkrp_f64(int N, uint64_t nnz, const float* vals,
                     const uint32_t* const* idx, int n, int R, int Rp,
                     const float* const* Y, double* out, uint32_t I_n)
 {
-    std::memset(out, 0, (size_t)I_n * Rp * sizeof(double));
-    std::vector<double> t(R);
-    for (uint64_t i = 0; i < nnz; ++i) {
-        const double v = vals[i];
-        for (int r = 0; r < R; ++r) t[r] = v;
-        for (int w = 0; w < N; ++w) {
-            if (w == n) continue;
-            const float* yw = Y[w] + (size_t)idx[w][i] * Rp;
-            for (int r = 0; r < R; ++r) t[r] *= (double)yw[r];
+    // rows in parallel over a stable row grouping of the nonzeros: each row
+    // adds its terms in nonzero order, as a serial loop over the nonzeros
+    // would, so the result does not depend on the thread count
+    std::vector<uint64_t> rp((size_t)I_n + 1, 0);
+    for (uint64_t i = 0; i < nnz; ++i) ++rp[(size_t)idx[n][i] + 1];
+    for (uint32_t r = 0; r < I_n; ++r) rp[r + 1] += rp[r];
+    std::vector<uint64_t> perm(nnz);
+    {
+        std::vector<uint64_t> cur(rp.begin(), rp.end() - 1);
+        for (uint64_t i = 0; i < nnz; ++i) perm[cur[idx[n][i]]++] = i;
+    }
+#pragma omp parallel
+    {
+        std::vector<double> t(R);
+#pragma omp for schedule(dynamic, 256)
+        for (int64_t row = 0; row < (int64_t)I_n; ++row) {
+            double* o = out + (size_t)row * Rp;
+            for (int r = 0; r < Rp; ++r) o[r] = 0.0;
+            for (uint64_t k = rp[row]; k < rp[row + 1]; ++k) {
+                const uint64_t i = perm[k];
+                const double v = vals[i];
+                for (int r = 0; r < R; ++r) t[r] = v;
+                for (int w = 0; w < N; ++w) {
+                    if (w == n) continue;
+                    const float* yw = Y[w] + (size_t)idx[w][i] * Rp;
+                    for (int r = 0; r < R; ++r) t[r] *= (double)yw[r];
+                }
+                for (int r = 0; r < R; ++r) o[r] += t[r];
+            }
         }
-        double* o = out + (size_t)idx[n][i] * Rp;
-        for (int r = 0; r < R; ++r) o[r] += t[r];
     }
 }
 
@@ -411,8 +431,15 @@ void orc_uniform_factors(uint64_t seed, int N, const uint32_t* dims, int R,
 int orc_cpals_f64(int N, uint64_t nnz, const uint32_t* dims, const float* vals,
                   const uint32_t* const* idx, int R, int Rp, int max_iters,
                   double tol, double ridge, float* const* Yio,
-                  double* fit_hist, double* lambda_out, int jacobi)
+                  double* fit_hist, double* lambda_out, int flags)
 {
+    // flags bit 0: Jacobi; bit 1: the MTTKRP gathers factor entries rounded
+    // to BF16 (round to nearest even, as a BF16 copy of FP32 factors holds
+    // them), everything else FP64 -- the arithmetic of BF16-gather CP-ALS
+    // without FP32 rounding
+    const int jacobi = flags & 1;
+    const bool bf16_any = (flags & 2) != 0;
+    const bool bf16_last_fp32 = (flags & 4) != 0;   // the last mode gathers FP32
     std::vector<std::vector<double>> Y(N), Yh(N), G(N);
     for (int n = 0; n < N; ++n) {
         Y[n].assign((size_t)dims[n] * R, 0);
@@ -421,31 +448,85 @@ int orc_cpals_f64(int N, uint64_t nnz, const uint32_t* dims, const float* vals,
         Yh[n].assign((size_t)dims[n] * R, 0);
         G[n].assign((size_t)R * R, 0);
     }
+    // Gram: partial sums over fixed 4096-row blocks, added in block order,
+    // so the result does not depend on the OpenMP thread count
     auto gram = [&](int n) {
+        const uint32_t I = dims[n];
+        const uint32_t nb = (I + 4095) / 4096;
+        std::vector<double> part((size_t)nb * R * R, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t blk = 0; blk < (int64_t)nb; ++blk) {
+            double* g = &part[(size_t)blk * R * R];
+            const uint32_t i1 = std::min<uint32_t>(I, (uint32_t)(blk + 1) * 4096);
+            for (uint32_t i = (uint32_t)blk * 4096; i < i1; ++i) {
+                const double* y = &Y[n][(size_t)i * R];
+                for (int a = 0; a < R; ++a)
+                    for (int b = 0; b < R; ++b) g[a * R + b] += y[a] * y[b];
+            }
+        }
         std::fill(G[n].begin(), G[n].end(), 0.0);
-        for (uint32_t i = 0; i < dims[n]; ++i)
-            for (int a = 0; a < R; ++a)
-                for (int b = 0; b < R; ++b)
-                    G[n][a * R + b] += Y[n][(size_t)i * R + a] * Y[n][(size_t)i * R + b];
+        for (uint32_t blk = 0; blk < nb; ++blk)
+            for (int a = 0; a < R * R; ++a) G[n][a] += part[(size_t)blk * R * R + a];
     };
     for (int n = 0; n < N; ++n) gram(n);
     double tn2 = 0;
     for (uint64_t i = 0; i < nnz; ++i) tn2 += (double)vals[i] * vals[i];
     const double tn = std::sqrt(tn2);
-    std::vector<double> lam(R, 1.0), V((size_t)R * R), t(R);
+    std::vector<double> lam(R, 1.0), V((size_t)R * R);
     double fit_prev = 0;
     int it = 0;
+    // Row-grouped nonzero lists per mode (a stable counting sort by the
+    // mode's index), so rows are summed in parallel without races and each
+    // row's terms are added in the input's nonzero order whatever the
+    // thread count.
+    std::vector<std::vector<uint64_t>> rp(N);
+    std::vector<std::vector<uint32_t>> perm(N);
+    for (int n = 0; n < N; ++n) {
+        rp[n].assign((size_t)dims[n] + 1, 0);
+        for (uint64_t i = 0; i < nnz; ++i) ++rp[n][(size_t)idx[n][i] + 1];
+        for (uint32_t r = 0; r < dims[n]; ++r) rp[n][r + 1] += rp[n][r];
+        perm[n].resize(nnz);
+        std::vector<uint64_t> cur(rp[n].begin(), rp[n].end() - 1);
+        for (uint64_t i = 0; i < nnz; ++i) perm[n][cur[idx[n][i]]++] = (uint32_t)i;
+    }
+    std::vector<std::vector<double>> Yg(N);    // gathered copies (BF16-rounded)
+    auto to_bf16 = [](double x) -> double {
+        float f = (float)x;
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        if ((u & 0x7f800000u) != 0x7f800000u) u += 0x7fffu + ((u >> 16) & 1u);
+        u &= 0xffff0000u;
+        std::memcpy(&f, &u, 4);
+        return (double)f;
+    };
     auto mttkrp = [&](int n) {
-        std::fill(Yh[n].begin(), Yh[n].end(), 0.0);
-        for (uint64_t i = 0; i < nnz; ++i) {
-            for (int r = 0; r < R; ++r) t[r] = vals[i];
+        const bool bf16 = bf16_any && !(bf16_last_fp32 && n == N - 1);
+        if (bf16)
             for (int w = 0; w < N; ++w) {
                 if (w == n) continue;
-                const double* y = &Y[w][(size_t)idx[w][i] * R];
-                for (int r = 0; r < R; ++r) t[r] *= y[r];
+                Yg[w].resize(Y[w].size());
+                // the FP32 master copy is what the device rounds to BF16
+                for (size_t k = 0; k < Y[w].size(); ++k) Yg[w][k] = to_bf16((float)Y[w][k]);
             }
-            double* o = &Yh[n][(size_t)idx[n][i] * R];
-            for (int r = 0; r < R; ++r) o[r] += t[r];
+        const std::vector<std::vector<double>>& Ys = bf16 ? Yg : Y;
+#pragma omp parallel
+        {
+            std::vector<double> t(R);
+#pragma omp for schedule(dynamic, 256)
+            for (int64_t row = 0; row < (int64_t)dims[n]; ++row) {
+                double* o = &Yh[n][(size_t)row * R];
+                for (int r = 0; r < R; ++r) o[r] = 0.0;
+                for (uint64_t k = rp[n][row]; k < rp[n][row + 1]; ++k) {
+                    const uint32_t i = perm[n][k];
+                    for (int r = 0; r < R; ++r) t[r] = vals[i];
+                    for (int w = 0; w < N; ++w) {
+                        if (w == n) continue;
+                        const double* y = &Ys[w][(size_t)idx[w][i] * R];
+                        for (int r = 0; r < R; ++r) t[r] *= y[r];
+                    }
+                    for (int r = 0; r < R; ++r) o[r] += t[r];
+                }
+            }
         }
     };
     for (; it < max_iters; ++it) {
@@ -476,7 +557,8 @@ int orc_cpals_f64(int N, uint64_t nnz, const uint32_t* dims, const float* vals,
                     V[i * R + j] = q * inv;
                 }
             }
-            for (uint32_t i = 0; i < dims[n]; ++i) {   // row solves
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < (int64_t)dims[n]; ++i) {   // row solves
                 double* x = &Y[n][(size_t)i * R];
                 const double* b = &Yh[n][(size_t)i * R];
                 for (int r = 0; r < R; ++r) x[r] = b[r];

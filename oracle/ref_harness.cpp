@@ -354,4 +354,23 @@ void* ref_load_dnp(const char* path, int threads, int quiet)
     return h;
 }
 
+// dyn_build_compute_plan on the built tensor (src/dynasor_preprocess.cpp:
+// 1179-1363): the CP-ALS kernel it picks (0 GS, 1 Jacobi), its reason and
+// the per-mode kernel class (0 Element, 1 Fiber, 2 FiberCSR).  layout is
+// the layout the tensor was built with ("pingpong" | "ncopy").
+int ref_compute_plan(void* hp, int rank_padded, int threads, const char* layout,
+                     const char* kernel_cli, char* reason, int reason_cap, int* per_mode)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    ComputePlan p;
+    {
+        Quiet q(h->quiet);
+        p = dyn_build_compute_plan(h->T, rank_padded, threads, layout ? layout : "",
+                                   "off", kernel_cli ? kernel_cli : "");
+    }
+    if (reason && reason_cap > 0) std::snprintf(reason, (size_t)reason_cap, "%s", p.kernel_reason);
+    for (int n = 0; n < h->T.num_modes; ++n) per_mode[n] = (int)p.per_mode[n];
+    return p.kernel_enum;
+}
+
 } // extern "C"

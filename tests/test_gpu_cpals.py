@@ -45,11 +45,25 @@ def test_fit_and_factors_match_fp64_oracle(bindings, overlap, monkeypatch):
 
 
 def test_bf16_gather_cpals_within_tolerance_of_fp64(bindings):
+    """BF16 gathers (the last mode's MTTKRP in FP32, which keeps the fit's
+    <X, M> term exact up to FP32): final fit within the north-star 1e-4 of
+    FP64 CP-ALS, and every fit within 1e-6 of the FP64 run whose MTTKRP
+    reads the same BF16-rounded factors.  (With every mode in BF16 the FP64
+    emulation already misses 1e-4 on this tensor: 2.1e-4.)"""
     g, dims, idx, p = _golden_plan(precision="bf16")
     it, R = int(g["iters"]), int(g["R"])
     r = p.cpals(max_iters=it, tol=0.0, seed=42)
-    fit64, _, _ = bindings.cpals_f64(dims, g["vals"], idx, R, it, 0.0, seed=42)
-    assert abs(r["final_fit"] - fit64[-1]) < 1e-3
+    fit64, Y64, _ = bindings.cpals_f64(dims, g["vals"], idx, R, it, 0.0, seed=42)
+    fitb, _, _ = bindings.cpals_f64(dims, g["vals"], idx, R, it, 0.0, seed=42,
+                                    bf16_gathers=True, last_mode_fp32=True)
+    h = r["fit_history"]
+    ef = [rel_fro(p.factor(n)[:, :R], Y64[n][:, :R]) for n in range(len(dims))]
+    print(f"\nBF16 CP-ALS: final fit {h[-1]:.8f} vs FP64 {fit64[-1]:.8f} "
+          f"(|d| {abs(h[-1] - fit64[-1]):.2e}, max over iterations "
+          f"{np.max(np.abs(h - fit64)):.2e}); vs BF16-rounded FP64 {np.max(np.abs(h - fitb)):.2e}; "
+          "factor rel-Fro vs FP64 " + " ".join(f"{e:.2e}" for e in ef))
+    assert abs(h[-1] - fit64[-1]) < FIT_TOL
+    assert np.max(np.abs(h - fitb)) < 1e-6
 
 
 def test_convergence_stop_rule():
@@ -156,11 +170,22 @@ def test_four_mode_bf16_rank64_against_fp64_oracle(bindings, kernel):
     R, it = 64, (3 if kernel == "gs" else 2)
     p = d.Plan(dims, vals, idx, threads=8, rank=R, precision="bf16")
     r = p.cpals(max_iters=it, tol=0.0, seed=42, kernel=kernel)
-    fit64, Y64, lam64 = bindings.cpals_f64(dims, vals, idx, R, it, 0.0, seed=42,
-                                           jacobi=(kernel == "jacobi"))
-    assert np.max(np.abs(r["fit_history"] - fit64)) < 1e-3
-    for n in range(len(dims)):
-        assert rel_fro(p.factor(n)[:, :R], Y64[n][:, :R]) < 5e-2
+    jac = kernel == "jacobi"
+    fit64, Y64, lam64 = bindings.cpals_f64(dims, vals, idx, R, it, 0.0, seed=42, jacobi=jac)
+    fitb, Yb, _ = bindings.cpals_f64(dims, vals, idx, R, it, 0.0, seed=42, jacobi=jac,
+                                     bf16_gathers=True, last_mode_fp32=True)
+    e64 = [rel_fro(p.factor(n)[:, :R], Y64[n][:, :R]) for n in range(len(dims))]
+    eb = [rel_fro(p.factor(n)[:, :R], Yb[n][:, :R]) for n in range(len(dims))]
+    df = float(np.max(np.abs(r["fit_history"] - fit64)))
+    print(f"\n4-mode BF16 rank 64 {kernel}: max |dfit| vs FP64 {df:.2e}; factor rel-Fro vs FP64 "
+          + " ".join(f"{e:.2e}" for e in e64) + "; vs BF16-rounded FP64 "
+          + " ".join(f"{e:.2e}" for e in eb))
+    # BF16 rounding of the gathered factors moves the factors by ~5e-3
+    # (GS, 3 iterations) and ~7e-3 (Jacobi, 2) against FP64, the fit by
+    # < 1e-6; the same rounding in FP64 leaves only FP32 accumulation
+    assert df < FIT_TOL
+    assert max(e64) < 1.5e-2
+    assert max(eb) < 1e-4
     p.close()
 
 
