@@ -24,9 +24,14 @@
 //      host threads on one device) race on the array: serialise them;
 //    * the first call on a device looks up the array's device address
 //      (cudaGetSymbolAddress with that device current) and caches it; make
-//      that first call before any stream capture;
+//      that first call before any stream capture.  The cached address is
+//      not looked up again, so cudaDeviceReset on that device after the
+//      first call is not supported (the array would move with the new
+//      context);
 //    * the call waits for its own stream once at the end to read the fault
-//      flag (keys >= num_buckets are reported, never written out of range).
+//      flag (keys >= num_buckets are reported, never written out of range),
+//      so a call on a stream that is being captured is rejected with
+//      DGPU_ERR_ARG before any work is queued.
 //
 //  The kernels below are separate copies specialised for an input taken in
 //  slab order (tile t = [t*4096, ...)), so no tile table is needed.
@@ -283,13 +288,22 @@ extern "C" int dgpu_sort_slab_noalloc(void* stream, int num_modes, uint64_t nnz,
         in.idx[n] = idx_in[n];
         out.idx[n] = idx_out[n];
     }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the call ends with a blocking read of the fault flag, which a stream
+    // capture cannot hold
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    DGPU_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+        set_error("dgpu_sort_slab_noalloc: the stream is being captured; this call waits for "
+                  "its stream and reads a status back, so call it outside a capture");
+        return DGPU_ERR_ARG;
+    }
     uint32_t* base = nullptr;
     DGPU_TRY(na_scratch(&base));
     uint32_t* cnt = base;
     uint32_t* off = base + kMaxEntries;
     uint32_t* aux = base + 2 * kMaxEntries;
     uint32_t* flag = aux + kAuxWords - 1;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     DGPU_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
     k_na_hist<<<ntiles, kNaThreads, num_buckets * sizeof(uint32_t), st>>>(

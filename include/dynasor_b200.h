@@ -402,8 +402,10 @@ int dgpu_cpopt_gradient(dgpu_plan* plan, float* const* grad_host);
  * ceil(nnz / 4096)) are rejected with DGPU_ERR_ARG.  Calls share that
  * array, so calls whose device work overlaps race; the first call on a
  * device resolves the array's address and should come before any stream
- * capture.  Waits for `stream` before returning; a key >= num_buckets
- * yields DGPU_ERR_INDEX. */
+ * capture, and that address is kept (cudaDeviceReset on the device after
+ * the first call is not supported).  Waits for `stream` before returning,
+ * so a call on a stream that is being captured gives DGPU_ERR_ARG; a key
+ * >= num_buckets yields DGPU_ERR_INDEX. */
 int dgpu_sort_slab_noalloc(void* stream, int num_modes, uint64_t nnz,
                            const float* vals_in, const uint32_t* const* idx_in,
                            float* vals_out, uint32_t* const* idx_out,

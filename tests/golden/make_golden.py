@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference tree>   (or REF=<tree>)
 
 Drives the UNMODIFIED reference sources compiled by oracle/Makefile
 (oracle/_ref/libdynref_*.so) through their own API -- build_flycoo,
@@ -103,7 +103,8 @@ def cpals_case(dims, vals, idx, T, R, iters, tol):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("REF"), required="REF" not in os.environ,
+                    help="the reference source tree (or set REF)")
     a = ap.parse_args()
     if not B.ref_available():
         sys.exit("oracle/_ref is not built; run `make -C oracle ref` first")

@@ -53,6 +53,22 @@ def test_noalloc_partition_matches_plan_build_twice():
             assert np.array_equal(ix[n], ref_i[n]), (call, n)
 
 
+def test_noalloc_multi_block_scan_matches_stable_argsort():
+    """~1M nonzeros in 2048 buckets: 245 tiles x 2048 buckets = 501,760
+    counters, 31 blocks of the counter scan (the block sums are scanned and
+    added back), against numpy's stable argsort by key, twice in a row."""
+    from dynasor_plus_b200 import synth
+    shift = 3
+    dims, vals, idx = synth.uniform((2048 << shift, 300, 200), 1_000_000, seed=81)
+    key = idx[0] >> shift
+    order = np.argsort(key, kind="stable")
+    for _ in range(2):
+        v, ix = _sort_noalloc(vals, idx, 0, shift, 2048)
+        assert np.array_equal(v, vals[order])
+        for n in range(3):
+            assert np.array_equal(ix[n], idx[n][order]), n
+
+
 def test_noalloc_rejects_oversized_and_bad_keys():
     import dynasor_plus_b200 as d
     from dynasor_plus_b200 import synth
@@ -68,3 +84,29 @@ def test_noalloc_rejects_oversized_and_bad_keys():
     with pytest.raises(d.DgpuError) as e:
         _sort_noalloc(vals, idx, 0, 1, 2048)
     assert e.value.code == -1 and "scratch" in str(e.value)
+
+
+def test_noalloc_rejects_a_capturing_stream():
+    """The call ends with a blocking read of its fault flag, which a stream
+    capture cannot hold: on a capturing stream it queues nothing and gives
+    DGPU_ERR_ARG."""
+    import torch
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.uniform((64, 50, 20), 3000, seed=3)
+    vin = torch.from_numpy(vals).cuda()
+    iin = [torch.from_numpy(i.view(np.int32)).cuda() for i in idx]
+    vout = torch.empty_like(vin)
+    iout = [torch.empty_like(x) for x in iin]
+    pin = (C.c_void_p * 3)(*[x.data_ptr() for x in iin])
+    pout = (C.c_void_p * 3)(*[x.data_ptr() for x in iout])
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        rc = d.lib().dgpu_sort_slab_noalloc(C.c_void_p(s.cuda_stream), 3, len(vals),
+                                            C.c_void_p(vin.data_ptr()), pin,
+                                            C.c_void_p(vout.data_ptr()), pout, 0, 0, 64)
+        vout.add_(0.0)                      # keep the captured graph non-empty
+    assert rc == -1
+    assert b"captured" in d.lib().dgpu_last_error()
