@@ -30,12 +30,15 @@
 #include "apply_map.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <random>
 #include <memory>
+#include <mutex>
+#include <random>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -371,13 +374,20 @@ k_gram_partial(const float* __restrict__ Y, uint32_t rows, int R, int Rp,
 // Launches k_gram_partial (its shared memory is above the 48 KB default).
 int launch_gram_partial(dim3 grid, cudaStream_t st, const float* Y, uint32_t rows, int R, int Rp,
                         double* partial) {
+    // once per device (function attributes are per context); batched runs
+    // set up several plans on parallel host threads
+    static std::mutex mu;
     static bool attr_set[64] = {};
     int dev = 0;
     DGPU_CUDA(cudaGetDevice(&dev));
-    if (!attr_set[dev & 63]) {
-        DGPU_CUDA(cudaFuncSetAttribute(k_gram_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kGramSmem));
-        attr_set[dev & 63] = true;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!attr_set[dev & 63]) {
+            DGPU_CUDA(cudaFuncSetAttribute(k_gram_partial,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kGramSmem));
+            attr_set[dev & 63] = true;
+        }
     }
     k_gram_partial<<<grid, kLaThreads, kGramSmem, st>>>(Y, rows, R, Rp, partial);
     DGPU_CUDA(cudaGetLastError());
@@ -1030,15 +1040,22 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
 // (src/dynasor_cpals.cpp:42-69): a splitmix64 step of (seed, n) seeds a
 // std::mt19937_64, entries from std::normal_distribution<float>(0, 1),
 // row-major, padding zero.  Generated on the host, uploaded once.
-int init_factors_host(Plan& p, uint64_t seed) {
+// skip_mode >= 0: that mode's factor is zeroed instead of drawn.  Each mode
+// has its own generator, so the other modes' draws are unchanged;
+// Gauss-Seidel never reads mode 0's initial factor (mode 0 is solved first,
+// from the other modes' Grams, and its Gram is recomputed from the result),
+// so a Gauss-Seidel run skips the draw of mode 0 -- on the 1M-row rank-32
+// factor, 32M normal draws.
+int init_factors_host(Plan& p, uint64_t seed, int skip_mode) {
     // one independent generator per mode: draw the modes on parallel host
     // threads (large factors take seconds to draw serially)
     std::vector<std::vector<float>> Y(p.N);
     std::vector<std::thread> th;
     size_t total = 0;
-    for (int n = 0; n < p.N; ++n) total += (size_t)p.dims[n] * p.R;
+    for (int n = 0; n < p.N; ++n) total += n == skip_mode ? 0 : (size_t)p.dims[n] * p.R;
     const bool par = total >= (1u << 20);       // small factors: no thread start-up
     for (int n = 0; n < p.N; ++n) {
+        if (n == skip_mode) continue;
         auto draw = [&, n]() {
             uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
             z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
@@ -1055,8 +1072,11 @@ int init_factors_host(Plan& p, uint64_t seed) {
     }
     for (auto& t : th) t.join();
     for (int n = 0; n < p.N; ++n) {
-        DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y[n].data(), Y[n].size() * sizeof(float),
-                                  cudaMemcpyHostToDevice, p.stream));
+        if (n == skip_mode)
+            DGPU_CUDA(cudaMemsetAsync(p.Y[n], 0, (size_t)p.dims[n] * p.Rp * sizeof(float), p.stream));
+        else
+            DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y[n].data(), Y[n].size() * sizeof(float),
+                                      cudaMemcpyHostToDevice, p.stream));
         p.yb_stale[n] = true;
     }
     DGPU_CUDA(cudaStreamSynchronize(p.stream));
@@ -1111,6 +1131,7 @@ struct CpSession {
     bool done = false;
     bool graphs = false;
     clk::time_point t_start;
+    clk::time_point t_it;                    // start of the iteration in flight
     // host plan state saved around a capture (a capture advances it without
     // running the work)
     int cur0 = 0, nm0 = 0;
@@ -1134,7 +1155,8 @@ struct CpSession {
     int setup() {
         res = dgpu_cp_result{};
         DGPU_TRY(la_ensure(p, L));
-        if (!o.use_init) DGPU_TRY(init_factors_host(p, o.seed));
+        const bool gs = o.kernel != DGPU_CP_JACOBI && p.layout != DGPU_LAYOUT_MORTON;
+        if (!o.use_init) DGPU_TRY(init_factors_host(p, o.seed, gs && o.max_iters > 0 ? 0 : -1));
         for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
         // ||T||^2 of the plan's values, computed once per plan
         if (p.cp_tnorm2 < 0.0) DGPU_TRY(cp_tensor_norm(p, live_vals(p), &p.cp_tnorm2));
@@ -1254,7 +1276,14 @@ struct CpSession {
     // per-iteration graph keyed by the live slab (PingPong alternates slabs,
     // so at most two graphs), then the fit bookkeeping and the stop rule.
     int step_host() {
-        const auto t_it = clk::now();
+        DGPU_TRY(launch_iteration());
+        return collect_iteration();
+    }
+
+    // The iteration's work on p.stream, not waited for (a batch launches the
+    // first iterations of all its plans before it collects any).
+    int launch_iteration() {
+        t_it = clk::now();
         const int key = (p.layout == DGPU_LAYOUT_NCOPY) ? 0 : (p.cur & 1);
         if (graphs && it > 0 && exec[key]) {
             DGPU_CUDA(cudaGraphLaunch(exec[key], p.stream));
@@ -1288,6 +1317,11 @@ struct CpSession {
         } else {
             DGPU_TRY(enqueue(0));
         }
+        return DGPU_OK;
+    }
+
+    // Waits for the launched iteration; fit bookkeeping and the stop rule.
+    int collect_iteration() {
         DGPU_CUDA(cudaStreamSynchronize(p.stream));
         float mt_ms = 0.f, la_ms = 0.f;
         for (int n = 0; n < p.N; ++n) {
@@ -1436,10 +1470,41 @@ struct CpSession {
     }
 };
 
+// Key of a batch's loop graph: the plans (by serial, never reused) and each
+// session's loop key, in batch order.
+std::vector<uint64_t> batch_key(const std::vector<CpSession*>& ss) {
+    std::vector<uint64_t> key{(uint64_t)ss.size()};
+    for (CpSession* s : ss) {
+        uint64_t k[12];
+        s->loop_key(k);
+        key.push_back(s->p.serial);
+        key.insert(key.end(), k, k + 12);
+    }
+    return key;
+}
+
+// Launches `gx` on `launch` and hands every session its share of the loop.
+int launch_loops(std::vector<CpSession*>& in, cudaGraphExec_t gx, cudaStream_t launch) {
+    cudaEvent_t a, b;
+    DGPU_CUDA(cudaEventCreate(&a));
+    DGPU_CUDA(cudaEventCreate(&b));
+    struct E { cudaEvent_t a, b; ~E() { cudaEventDestroy(a); cudaEventDestroy(b); } } eg{a, b};
+    DGPU_CUDA(cudaEventRecord(a, launch));
+    DGPU_CUDA(cudaGraphLaunch(gx, launch));
+    DGPU_CUDA(cudaEventRecord(b, launch));
+    DGPU_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    for (CpSession* s : in) DGPU_TRY(s->finish_loop(ms));
+    return DGPU_OK;
+}
+
 // Runs the device loops of `ss` (all eligible) as parallel WHILE nodes of one
-// graph, launched once on `launch`.  Sessions whose capture is not possible
-// are left to iterate from the host.
-int run_loops(std::vector<CpSession*>& ss, cudaStream_t launch) {
+// graph, launched once on `owner`'s stream.  Sessions whose capture is not
+// possible are left to iterate from the host.  When every session is in the
+// graph it is kept on `owner` with the batch key, for a later call on the
+// same plans (cpals_batch_run).
+int run_loops(std::vector<CpSession*>& ss, Plan& owner) {
     cudaGraph_t outer = nullptr;
     cudaGraphExec_t gx = nullptr;
     struct G { cudaGraph_t& g; cudaGraphExec_t& x;
@@ -1468,19 +1533,14 @@ int run_loops(std::vector<CpSession*>& ss, cudaStream_t launch) {
         for (CpSession* s : in) { s->restore_state(); s->graphs = false; }
         return DGPU_OK;
     }
-    cudaEvent_t a, b;
-    DGPU_CUDA(cudaEventCreate(&a));
-    DGPU_CUDA(cudaEventCreate(&b));
-    DGPU_CUDA(cudaEventRecord(a, launch));
-    DGPU_CUDA(cudaGraphLaunch(gx, launch));
-    DGPU_CUDA(cudaEventRecord(b, launch));
-    DGPU_CUDA(cudaEventSynchronize(b));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    for (CpSession* s : in) DGPU_TRY(s->finish_loop(ms));
-    return DGPU_OK;
+    if (in.size() == ss.size()) {
+        if (owner.cp_batch_exec) cudaGraphExecDestroy(owner.cp_batch_exec);
+        owner.cp_batch_exec = gx;
+        owner.cp_batch_key = batch_key(in);
+        gx = nullptr;                            // kept: not destroyed with the guard
+        return launch_loops(in, owner.cp_batch_exec, owner.stream);
+    }
+    return launch_loops(in, gx, owner.stream);
 }
 
 // The device loop of one run, with its executable graph kept on the plan:
@@ -1558,25 +1618,72 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
     return DGPU_OK;
 }
 
-// Independent CP-ALS runs on several plans (one per tensor) whose remaining
-// iterations run as parallel device loops of one graph launch.
+// Independent CP-ALS runs on several plans (one per tensor).
+//   * The set-up of every run (initial factors drawn on the host, Grams,
+//     ||T||^2) runs on parallel host threads, one plan each.
+//   * A batch whose loop graph is kept on plans[0] for these plans and
+//     options runs every iteration, the first included, in one launch of
+//     that graph (the eager first iteration's allocations and tuning were
+//     done by the call that captured it).
+//   * Otherwise every plan's first iteration is launched on its own stream
+//     before any is waited for, then the remaining iterations run as
+//     parallel device loops of one graph launch, and that graph is kept.
 int cpals_batch_run(Plan* const* plans, int count, const dgpu_cp_options& o,
                     dgpu_cp_result* res, double* fit_history) {
     std::vector<std::unique_ptr<CpSession>> ss;
-    for (int k = 0; k < count; ++k) {
+    for (int k = 0; k < count; ++k)
         ss.emplace_back(new CpSession(*plans[k], o, res[k],
                                       fit_history ? fit_history + (size_t)k * std::max(1, o.max_iters)
                                                   : nullptr));
-        CpSession& s = *ss.back();
-        DGPU_CUDA(cudaSetDevice(plans[k]->device));
-        DGPU_TRY(s.setup());
-        if (!s.done) DGPU_TRY(s.step_host());
+    {
+        std::vector<int> rc(count, DGPU_OK);
+        std::vector<std::string> msg(count);
+        std::atomic<int> next{0};
+        const int nth = std::max(1, std::min<int>(count, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 0; t < nth; ++t)
+            th.emplace_back([&]() {
+                for (int k = next++; k < count; k = next++) {
+                    if (cudaSetDevice(plans[k]->device) != cudaSuccess) {
+                        rc[k] = DGPU_ERR_CUDA;
+                        msg[k] = "cudaSetDevice failed";
+                        continue;
+                    }
+                    rc[k] = ss[k]->setup();
+                    if (rc[k] != DGPU_OK) msg[k] = last_error();
+                }
+            });
+        for (auto& t : th) t.join();
+        DGPU_CUDA(cudaSetDevice(plans[0]->device));
+        for (int k = 0; k < count; ++k)
+            if (rc[k] != DGPU_OK) {
+                set_error("cpals batch, plan %d: %s", k, msg[k].c_str());
+                return rc[k];
+            }
     }
-    std::vector<CpSession*> loop;
-    for (auto& s : ss)
-        if (s->loop_eligible()) loop.push_back(s.get());
-    if (!loop.empty()) DGPU_TRY(run_loops(loop, plans[0]->stream));
-    for (auto& s : ss) {
+    std::vector<CpSession*> all;
+    for (auto& s : ss) all.push_back(s.get());
+    Plan& owner = *plans[0];
+    bool cached = owner.cp_batch_exec != nullptr && !o.verbose;
+    for (CpSession* s : all) cached = cached && s->graphs && !s->done;
+    if (cached) {
+        for (CpSession* s : all) DGPU_TRY(s->ensure_state());
+        cached = owner.cp_batch_exec != nullptr && batch_key(all) == owner.cp_batch_key;
+    }
+    if (cached) {
+        for (CpSession* s : all) DGPU_TRY(s->write_state());
+        DGPU_TRY(launch_loops(all, owner.cp_batch_exec, owner.stream));
+    } else {
+        for (CpSession* s : all)
+            if (!s->done) DGPU_TRY(s->launch_iteration());
+        for (CpSession* s : all)
+            if (!s->done) DGPU_TRY(s->collect_iteration());
+        std::vector<CpSession*> loop;
+        for (CpSession* s : all)
+            if (s->loop_eligible()) loop.push_back(s);
+        if (!loop.empty()) DGPU_TRY(run_loops(loop, owner));
+    }
+    for (CpSession* s : all) {
         while (!s->done) DGPU_TRY(s->step_host());
         s->finish();
     }
@@ -1632,35 +1739,57 @@ k_grad_rows(const float* __restrict__ Y, const float* __restrict__ Yhat, uint32_
 int cpopt_gradient(Plan& p, float* const* grad_host) {
     LaLayout L{};
     DGPU_TRY(la_ensure(p, L));
-    DGPU_TRY(launch_mttkrp_all_modes(p));
+    // MTTKRP_n for every n from one factor snapshot.  The mode passes keep
+    // each output row in registers; the all-modes pass adds every nonzero to
+    // N output rows with vector atomics, which piles up on short modes (a
+    // 1,000-row mode of a 20M-nonzero tensor takes 20,000 atomics per row).
+    // NCopy plans and PingPong plans between sweeps run the mode passes (a
+    // PingPong sweep leaves the slab primed for mode 0 again, in the order
+    // the reference's next sweep would have); otherwise, and on Morton
+    // plans, the all-modes pass.  Gathers are FP32 whatever the plan's
+    // precision: this is a gradient check path, not a BF16 one.
+    p.gather_fp32_all = true;
+    struct Reset { Plan& p; ~Reset() { p.gather_fp32_all = false; } } reset{p};
+    if (p.layout == DGPU_LAYOUT_NCOPY) {
+        for (int n = 0; n < p.N; ++n) DGPU_TRY(mode_ncopy(p, n));
+    } else if (p.layout == DGPU_LAYOUT_PINGPONG && p.next_mode == 0) {
+        for (int n = 0; n < p.N; ++n) DGPU_TRY(mode_pingpong(p, n));
+        DGPU_TRY(pingpong_drain(p));
+    } else {
+        DGPU_TRY(launch_mttkrp_all_modes(p));
+    }
     for (int n = 0; n < p.N; ++n) DGPU_TRY(gram_into(p, L, n, 0));
-    float* g = nullptr;
-    size_t gmax = 0;
-    for (int n = 0; n < p.N; ++n) gmax = std::max(gmax, (size_t)p.dims[n] * p.Rp);
-    DGPU_TRY(dev_alloc(p, (void**)&g, gmax * sizeof(float)));
-    int rc = DGPU_OK;
+    // one device buffer for all modes' gradients, kept on the plan
+    size_t total = 0;
+    for (int n = 0; n < p.N; ++n) total += (size_t)p.dims[n] * p.Rp;
+    if (p.grad_cap < total) {
+        dev_free(p.grad_buf);
+        p.device_bytes -= p.grad_cap * sizeof(float);
+        p.grad_buf = nullptr;
+        p.grad_cap = 0;
+        DGPU_TRY(dev_alloc(p, (void**)&p.grad_buf, total * sizeof(float)));
+        p.grad_cap = total;
+    }
     const size_t sm = (size_t)p.R * p.R * sizeof(double);
     if (sm > 48 * 1024 &&
         cudaFuncSetAttribute(k_grad_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
             cudaSuccess) {
+        cudaGetLastError();
         set_error("cpopt_gradient: rank %d needs %zu B of shared memory", p.R, sm);
-        rc = DGPU_ERR_ARG;
+        return DGPU_ERR_ARG;
     }
-    for (int n = 0; n < p.N && rc == DGPU_OK; ++n) {
+    size_t off = 0;
+    for (int n = 0; n < p.N; ++n) {
+        float* g = p.grad_buf + off;
         k_hadamard_others<<<4, 256, 0, p.stream>>>(L.Gd, p.N, n, p.R, L.Wd);
         k_grad_rows<<<grid_for((size_t)p.dims[n] * p.Rp), kLaThreads, sm, p.stream>>>(
             p.Y[n], p.Yhat[n], p.dims[n], p.R, p.Rp, L.Wd, g);
-        if (cudaGetLastError() != cudaSuccess ||
-            cudaMemcpyAsync(grad_host[n], g, (size_t)p.dims[n] * p.Rp * sizeof(float),
-                            cudaMemcpyDeviceToHost, p.stream) != cudaSuccess ||
-            cudaStreamSynchronize(p.stream) != cudaSuccess) {
-            set_error("cpopt_gradient: mode %d failed", n);
-            rc = DGPU_ERR_CUDA;
-        }
+        DGPU_CUDA(cudaGetLastError());
+        DGPU_CUDA(cudaMemcpyAsync(grad_host[n], g, (size_t)p.dims[n] * p.Rp * sizeof(float),
+                                  cudaMemcpyDeviceToHost, p.stream));
+        off += (size_t)p.dims[n] * p.Rp;
     }
-    dev_free(g);
-    p.device_bytes -= gmax * sizeof(float);
-    return rc;
+    return sync_checked(p);
 }
 
 }  // namespace dgpu

@@ -137,7 +137,14 @@ struct TimedLaunch {
     double      bytes;    // algorithmic bytes of the launch
 };
 
+// A number no other plan of this process has had (plan.cu): keys of cached
+// graphs that span several plans name their plans by it, so a graph built
+// for a plan that has since been destroyed can never match a new plan that
+// reuses its address.
+uint64_t next_plan_serial();
+
 struct Plan {
+    uint64_t                 serial = next_plan_serial();
     // ---- per-launch timing (dgpu_plan_set_timing) -----------------------
     bool                     timing = false;
     std::vector<TimedLaunch> pending;
@@ -205,6 +212,9 @@ struct Plan {
     // that mode's Yhat gives the fit's <X, M> term, and BF16-rounded gathers
     // there move the fit by up to ~2e-4 on small, well-fitted tensors.
     int          fp32_gather_mode = -1;
+    bool         gather_fp32_all = false;       // every mode gathers FP32 (gradient path)
+    float*       grad_buf = nullptr;            // CP-OPT gradients of all modes
+    size_t       grad_cap = 0;                  // floats in grad_buf
     uint32_t*    part_cnt = nullptr;            // [chunks x buckets] counts
     uint32_t*    part_off = nullptr;            // [chunks x buckets] in-segment prefixes
     size_t       part_cap = 0;                  // entries of each
@@ -228,6 +238,11 @@ struct Plan {
     std::vector<cudaEvent_t> cp_ev, cp_fork, cp_join;
     cudaGraphExec_t cp_loop_exec = nullptr;
     uint64_t     cp_loop_key[12] = {};
+    // the device loops of a multi-tensor batch led by this plan (the first
+    // of the batch): one graph of parallel WHILE nodes, kept with its key
+    // (every plan's serial and loop key) for a later call on the same plans
+    cudaGraphExec_t cp_batch_exec = nullptr;
+    std::vector<uint64_t> cp_batch_key;
     double       cp_tnorm2 = -1.0;              // ||T||^2 once computed (< 0: not yet)
     double       cp_mttkrp_frac = 0.5;          // MTTKRP share of an iteration, last measured
     // Morton layout: sorted keys and their values (the slabs are freed once

@@ -646,7 +646,8 @@ int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
         if (w != n && w != w0) { wl = w; break; }
     FacPtrs F{};
     for (int w = 0; w < p.N; ++w) { F.Y[w] = p.Y[w]; F.Yb[w] = p.Yb[w]; }
-    const bool bf = (p.precision == DGPU_PREC_BF16) && n != p.fp32_gather_mode;
+    const bool bf = (p.precision == DGPU_PREC_BF16) && n != p.fp32_gather_mode &&
+                    !p.gather_fp32_all;
     if (bf)
         for (int w = 0; w < p.N; ++w)
             if (w != n && p.yb_stale[w]) DGPU_TRY(launch_to_bf16(p, w));

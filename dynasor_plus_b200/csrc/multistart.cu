@@ -442,17 +442,21 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
 
     // ---- initial factors: restart k from seed + k, the reference's draw ---
     if (!o.use_init) {
-        // one generator per (mode, restart), drawn on parallel host threads
+        // one generator per (mode, restart), drawn on parallel host threads;
+        // Gauss-Seidel never reads mode 0's initial factor (it is solved
+        // first, from the other modes' Grams), so its draw is skipped and the
+        // factor zeroed -- the other draws are unchanged (own generators)
+        const int first = (o.kernel != DGPU_CP_JACOBI && max_iters > 0) ? 1 : 0;
         std::vector<std::vector<float>> Y(N);
-        for (int n = 0; n < N; ++n) Y[n].assign((size_t)p.dims[n] * p.Rp, 0.f);
-        const int jobs = N * K;
+        for (int n = first; n < N; ++n) Y[n].assign((size_t)p.dims[n] * p.Rp, 0.f);
+        const int jobs = (N - first) * K;
         const int nth = std::max(1, std::min<int>(jobs, (int)std::thread::hardware_concurrency()));
         std::atomic<int> next{0};
         std::vector<std::thread> th;
         for (int t = 0; t < nth; ++t)
             th.emplace_back([&]() {
                 for (int j = next++; j < jobs; j = next++) {
-                    const int n = j / K, k = j % K;
+                    const int n = first + j / K, k = j % K;
                     uint64_t z = (o.seed + (uint64_t)k) + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
                     z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
                     z ^= z >> 27; z *= 0x94D049BB133111EBULL;
@@ -466,8 +470,12 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
             });
         for (auto& t : th) t.join();
         for (int n = 0; n < N; ++n) {
-            DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y[n].data(), Y[n].size() * sizeof(float),
-                                      cudaMemcpyHostToDevice, p.stream));
+            if (n < first)
+                DGPU_CUDA(cudaMemsetAsync(p.Y[n], 0, (size_t)p.dims[n] * p.Rp * sizeof(float),
+                                          p.stream));
+            else
+                DGPU_CUDA(cudaMemcpyAsync(p.Y[n], Y[n].data(), Y[n].size() * sizeof(float),
+                                          cudaMemcpyHostToDevice, p.stream));
             p.yb_stale[n] = true;
         }
         DGPU_CUDA(cudaStreamSynchronize(p.stream));

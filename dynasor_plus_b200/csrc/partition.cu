@@ -39,6 +39,7 @@
 #include "dgpu_internal.h"
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 
 namespace dgpu {
@@ -661,16 +662,22 @@ int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, 
     const size_t smem = scatter_smem<N>(nb);
     // dynamic shared memory limit, raised per device (function attributes are
     // per context) to the largest request seen so far
+    // (the limit only grows; guarded because plans may be driven from
+    // several host threads)
+    static std::mutex mu;
     static size_t attr_bytes[64] = {};
-    size_t& have = attr_bytes[p.device & 63];
-    if (smem > have) {
-        if (smem > 227u * 1024u) {
-            set_error("stable_partition: %u buckets need %zu bytes of shared memory", nb, smem);
-            return DGPU_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        size_t& have = attr_bytes[p.device & 63];
+        if (smem > have) {
+            if (smem > 227u * 1024u) {
+                set_error("stable_partition: %u buckets need %zu bytes of shared memory", nb, smem);
+                return DGPU_ERR_ARG;
+            }
+            DGPU_CUDA(cudaFuncSetAttribute(k_chunk_scatter<N, W>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            have = smem;
         }
-        DGPU_CUDA(cudaFuncSetAttribute(k_chunk_scatter<N, W>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        have = smem;
     }
     int per_sm = 0;
     DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chunk_scatter<N, W>,

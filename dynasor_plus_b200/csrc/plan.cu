@@ -19,6 +19,8 @@
 // ============================================================================
 #include "dgpu_internal.h"
 
+#include <atomic>
+
 #include <algorithm>
 #include <functional>
 #include <cstdarg>
@@ -159,6 +161,11 @@ int timing_collect(Plan& p) {
     return DGPU_OK;
 }
 
+uint64_t next_plan_serial() {
+    static std::atomic<uint64_t> counter{1};
+    return counter.fetch_add(1);
+}
+
 Plan::~Plan() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
@@ -190,6 +197,8 @@ Plan::~Plan() {
     dev_free(mkeys);
     dev_free(mvals);
     if (cp_loop_exec) cudaGraphExecDestroy(cp_loop_exec);
+    if (cp_batch_exec) cudaGraphExecDestroy(cp_batch_exec);
+    dev_free(grad_buf);
     dev_free(cp_st);
     if (cp_fit_host) cudaFreeHost(cp_fit_host);
     for (auto e : cp_ev) cudaEventDestroy(e);

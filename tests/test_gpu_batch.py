@@ -44,3 +44,27 @@ def test_batch_rejects_repeated_plan():
     with pytest.raises(DgpuError):
         d.cpals_batch([p, p], max_iters=2)
     p.close()
+
+
+@pytest.mark.parametrize("layout", ["ncopy", "pingpong"])
+def test_repeated_batch_reuses_its_loop_graph(layout):
+    """The batch's loop graph is kept on its first plan: a second call with
+    the same options runs every iteration, the first included, in it; a call
+    with other options captures a new one; every call equals single runs."""
+    import dynasor_plus_b200 as d
+    ts = _tensors()
+    plans = [d.Plan(dims, v, i, threads=8, rank=8, layout=layout) for dims, v, i in ts]
+    want = {}
+    for tol in (1e-4, 1e-3):
+        want[tol] = []
+        for dims, v, i in ts:
+            q = d.Plan(dims, v, i, threads=8, rank=8, layout=layout)
+            want[tol].append(q.cpals(max_iters=40, tol=tol, seed=42))
+            q.close()
+    for tol in (1e-4, 1e-4, 1e-3, 1e-4, 1e-4):
+        got = d.cpals_batch(plans, max_iters=40, tol=tol, seed=42)
+        for k, r in enumerate(want[tol]):
+            assert got[k]["iters_done"] == r["iters_done"], (tol, k)
+            assert np.max(np.abs(got[k]["fit_history"] - r["fit_history"])) < 1e-6, (tol, k)
+    for p in plans:
+        p.close()
