@@ -24,7 +24,7 @@ import os
 import numpy as np
 
 from ._lib import (ComputePlan, ComputePlanInput, CpOptions, CpResult, Coo, DgpuError, DnpInfo,
-                   PlanInfo, PlanOpts, TensorDesc, check, lib, LIB_PATH)
+                   PlanInfo, PlanOpts, TensorDesc, TuneResult, check, lib, LIB_PATH)
 
 __all__ = ["Plan", "DgpuError", "cpals_batch", "padded_rank", "load_coo_tensor", "save_dnb_tensor",
            "dnp_peek",
@@ -407,6 +407,14 @@ class Plan:
                  "total_time_s": r.total_time_s,
                  "fit_history": hist[k, :r.iters_done].copy(),
                  "lambda": lam[k * Re:(k + 1) * Re].copy()} for k, r in enumerate(res)]
+
+    def autotune(self, sweeps: int = 2) -> dict:
+        """dgpu_plan_autotune: partition chunk sizes, digit widths and the
+        MTTKRP grid target chosen by timing whole sweeps (the slab advances
+        by the sweeps timed; no permutation depends on the knobs)."""
+        r = TuneResult()
+        check(lib().dgpu_plan_autotune(self._h, int(sweeps), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
 
     def compute_plan(self, kernel="auto") -> dict:
         """dyn_build_compute_plan for this plan: the CP-ALS kernel the

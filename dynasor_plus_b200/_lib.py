@@ -80,6 +80,13 @@ class ComputePlan(C.Structure):
                 ("budget_bytes", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("fiber_digit_bits", C.c_int), ("sort_digit_bits", C.c_int),
+                ("chunks_per_sm", C.c_int), ("seg_chunk_tiles", C.c_int),
+                ("mttkrp_ctas_per_sm", C.c_int), ("candidates", C.c_int),
+                ("default_ms", C.c_double), ("tuned_ms", C.c_double)]
+
+
 class KernelTiming(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("launches", C.c_uint64), ("total_ms", C.c_double),
                 ("bytes", C.c_double)]
@@ -107,6 +114,7 @@ _SIGS = {
     "dgpu_plan_sync": (C.c_int, [C.c_void_p]),
     "dgpu_plan_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "dgpu_plan_get_timing": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_int]),
+    "dgpu_plan_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TuneResult)]),
     "dgpu_plan_shards": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "dgpu_plan_schedule": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                      C.POINTER(C.c_uint32)]),

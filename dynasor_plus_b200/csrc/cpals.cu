@@ -1390,7 +1390,7 @@ struct CpSession {
 
     // What the captured loop body depends on: options, tensor norm, live
     // slab at the loop start and the device buffers it reads and writes.
-    void loop_key(uint64_t (&k)[12]) const {
+    void loop_key(uint64_t (&k)[kLoopKeyWords]) const {
         auto bits = [](double v) { uint64_t u; std::memcpy(&u, &v, 8); return u; };
         k[0] = (uint64_t)o.kernel;
         k[1] = (uint64_t)o.solve_fp64;
@@ -1404,6 +1404,7 @@ struct CpSession {
         k[9] = (uint64_t)(uintptr_t)st;
         k[10] = (uint64_t)(uintptr_t)p.lambda;
         k[11] = (uint64_t)(uintptr_t)p.Y[0];
+        k[12] = p.tables_gen;                  // partition lists and launch knobs
     }
 
     int capture_body(cudaGraph_t body, cudaGraphConditionalHandle h) {
@@ -1475,10 +1476,10 @@ struct CpSession {
 std::vector<uint64_t> batch_key(const std::vector<CpSession*>& ss) {
     std::vector<uint64_t> key{(uint64_t)ss.size()};
     for (CpSession* s : ss) {
-        uint64_t k[12];
+        uint64_t k[kLoopKeyWords];
         s->loop_key(k);
         key.push_back(s->p.serial);
-        key.insert(key.end(), k, k + 12);
+        key.insert(key.end(), k, k + kLoopKeyWords);
     }
     return key;
 }
@@ -1548,7 +1549,7 @@ int run_loops(std::vector<CpSession*>& ss, Plan& owner) {
 // state) instead of capturing and instantiating it again.
 int run_loop_cached(CpSession& s) {
     Plan& p = s.p;
-    uint64_t key[12];
+    uint64_t key[kLoopKeyWords];
     DGPU_TRY(s.ensure_state());
     s.loop_key(key);
     if (!p.cp_loop_exec || std::memcmp(key, p.cp_loop_key, sizeof(key)) != 0) {
@@ -1604,7 +1605,7 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
     bool replayed = false;
     if (s.graphs && !o.verbose && !s.done && p.cp_loop_exec) {
         DGPU_TRY(s.ensure_state());
-        uint64_t key[12];
+        uint64_t key[kLoopKeyWords];
         s.loop_key(key);
         if (std::memcmp(key, p.cp_loop_key, sizeof(key)) == 0) {
             DGPU_TRY(run_loop_cached(s));

@@ -143,6 +143,9 @@ struct TimedLaunch {
 // reuses its address.
 uint64_t next_plan_serial();
 
+// Words of a cached CP-ALS loop graph's key (cpals.cu, CpSession::loop_key).
+constexpr int kLoopKeyWords = 13;
+
 struct Plan {
     uint64_t                 serial = next_plan_serial();
     // ---- per-launch timing (dgpu_plan_set_timing) -----------------------
@@ -203,6 +206,12 @@ struct Plan {
     // second pass with narrow digits.
     int          sort_digit_bits = kDefaultDigitBits;
     int          fiber_digit_bits = kDefaultDigitBits;
+    // Chunk sizes of the partition passes and the MTTKRP grid target; the
+    // defaults were measured on the 64.7M-nonzero 3-mode tensor and
+    // dgpu_plan_autotune picks per plan.  Neither changes any permutation.
+    int          chunks_per_sm = 4;             // global (remap) partition: chunks per SM
+    int          seg_chunk_tiles = 16;          // segmented (fiber) partition: tiles per chunk
+    int          mttkrp_ctas_per_sm = 4;        // tiles are split until this many CTAs per SM
     float*       Y[kMaxModes] = {nullptr};
     float*       Yhat[kMaxModes] = {nullptr};
     __nv_bfloat16* Yb[kMaxModes] = {nullptr};
@@ -237,7 +246,10 @@ struct Plan {
     size_t       cp_st_bytes = 0;
     std::vector<cudaEvent_t> cp_ev, cp_fork, cp_join;
     cudaGraphExec_t cp_loop_exec = nullptr;
-    uint64_t     cp_loop_key[12] = {};
+    uint64_t     cp_loop_key[kLoopKeyWords] = {};
+    // bumped whenever the partition lists are rebuilt or a launch knob
+    // changes (dgpu_plan_autotune): part of every cached loop graph's key
+    uint64_t     tables_gen = 0;
     // the device loops of a multi-tensor batch led by this plan (the first
     // of the batch): one graph of parallel WHILE nodes, kept with its key
     // (every plan's serial and loop key) for a later call on the same plans
@@ -360,6 +372,9 @@ int fiber_sort(Plan& p, int n, int src, int other, int* result);
 // Build the chunk/segment tables of a tile list.  `seg_of_tile` (host, may
 // be empty) gives each tile's segment and `seg_base` each segment's output
 // start; empty means one global segment starting at 0.
+// Rebuilds every partition list of the plan with the current chunk sizes
+// (plan.cu).
+int plan_rebuild_partlists(Plan& p);
 int build_partlist(Plan& p, const std::vector<Tile>& tiles,
                    const std::vector<uint32_t>& seg_of_tile,
                    const std::vector<uint32_t>& seg_base, PartList& out, Tile* shared_tiles);

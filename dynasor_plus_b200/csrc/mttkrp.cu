@@ -493,8 +493,9 @@ int launch_rowrun(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
         if (F.Y[w]) F.Y[w] += c0;
         if (F.Yb[w]) F.Yb[w] += c0;
     }
-    // at least ~4 CTAs per SM: split tiles when the tensor has few of them
-    const uint32_t want = 4u * (uint32_t)p.sms;
+    // at least ~mttkrp_ctas_per_sm (default 4) CTAs per SM: split tiles
+    // when the tensor has few of them
+    const uint32_t want = (uint32_t)std::max(1, std::min(16, p.mttkrp_ctas_per_sm)) * (uint32_t)p.sms;
     const uint32_t split = ntiles >= want ? 1u : std::min(16u, (want + ntiles - 1) / std::max(1u, ntiles));
     const dim3 grid(ntiles, split);
 #define DGPU_RUNT(G, V, TN)                                                                      \

@@ -63,7 +63,7 @@ constexpr int kScatBufsMax = 3;
 // Thread that issues a scatter CTA's bulk copies: the last one, whose warp
 // has no bucket-prefix work for up to kScatThreads / 2 buckets.
 constexpr int kIssuer = kScatThreads - 1;
-constexpr uint32_t kSegChunkTiles = 16;       // <= 64K elements per segmented chunk
+constexpr uint32_t kSegChunkTilesMax = 16;    // <= 64K elements per segmented chunk
 
 __device__ __forceinline__ uint32_t part_key(uint32_t v, int shift, uint32_t mask) {
     return (v >> shift) & mask;
@@ -709,13 +709,15 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     std::vector<Chunk> ch;
     std::vector<Seg> sg;
     if (global) {
-        // 4 chunks per SM of near-equal element counts (cut where the running
-        // total crosses the next multiple of total / want), so the chunk
-        // count divides evenly over 1 or 2 resident scatter CTAs per SM
+        // chunks_per_sm (default 4) chunks per SM of near-equal element
+        // counts (cut where the running total crosses the next multiple of
+        // total / want), so the chunk count divides evenly over 1 or 2
+        // resident scatter CTAs per SM
         uint64_t total = 0;
         for (const Tile& t : tiles) total += t.count;
+        const uint64_t per_sm = (uint64_t)std::max(1, std::min(32, p.chunks_per_sm));
         const uint64_t want = std::max<uint64_t>(
-            1, std::min<uint64_t>(4ull * (uint64_t)p.sms, (total + kTile - 1) / kTile));
+            1, std::min<uint64_t>(per_sm * (uint64_t)p.sms, (total + kTile - 1) / kTile));
         Seg s{0, 0, 0, 0};
         uint32_t t0 = 0;
         uint64_t acc = 0;
@@ -730,6 +732,8 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
         s.chunk_end = (uint32_t)ch.size();
         sg.push_back(s);
     } else {
+        const uint32_t per_chunk = (uint32_t)std::max(
+            1, std::min((int)kSegChunkTilesMax, p.seg_chunk_tiles));
         const uint32_t nseg = (uint32_t)seg_base.size();
         sg.assign(nseg, Seg{0, 0, 0, 0});
         for (uint32_t s = 0; s < nseg; ++s) sg[s].base = seg_base[s];
@@ -738,7 +742,7 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
             sg[s].chunk_begin = (uint32_t)ch.size();
             while (t < tiles.size() && seg_of_tile[t] == s) {
                 const uint32_t t0 = t;
-                while (t < tiles.size() && seg_of_tile[t] == s && t - t0 < kSegChunkTiles) ++t;
+                while (t < tiles.size() && seg_of_tile[t] == s && t - t0 < per_chunk) ++t;
                 ch.push_back(Chunk{t0, t, s, 0});
             }
             sg[s].chunk_end = (uint32_t)ch.size();

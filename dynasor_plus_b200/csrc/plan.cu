@@ -493,6 +493,33 @@ static int plan_tables(Plan& p) {
     return build_partlist(p, id, kNone, kNone, p.ident, nullptr);
 }
 
+int plan_rebuild_partlists(Plan& p) {
+    static const std::vector<uint32_t> kNone;
+    // graphs captured over the old lists must not run again: drop this
+    // plan's, and bump the generation that every cached key carries (a
+    // batch graph kept on another plan then no longer matches)
+    ++p.tables_gen;
+    if (p.cp_loop_exec) { cudaGraphExecDestroy(p.cp_loop_exec); p.cp_loop_exec = nullptr; }
+    if (p.cp_batch_exec) { cudaGraphExecDestroy(p.cp_batch_exec); p.cp_batch_exec = nullptr; }
+    DGPU_CUDA(cudaStreamSynchronize(p.stream));
+    for (int n = 0; n < p.N; ++n) {
+        if (p.tiles_h[n].empty()) continue;
+        DGPU_TRY(build_partlist(p, p.tiles_h[n], kNone, kNone, p.proc[n], p.tiles_d[n]));
+        if (p.fib[n].chunks) DGPU_TRY(build_fiber_tiles(p, n));
+    }
+    if (!p.ident.chunks) return DGPU_OK;
+    std::vector<Tile> id;
+    for (uint64_t x = 0; x < p.nnz; x += kTile) {
+        Tile tl;
+        tl.begin = (uint32_t)x;
+        tl.count = (uint32_t)std::min<uint64_t>(kTile, p.nnz - x);
+        tl.shard = 0;
+        tl.seg_first = 0;
+        id.push_back(tl);
+    }
+    return build_partlist(p, id, kNone, kNone, p.ident, nullptr);
+}
+
 static int plan_factors(Plan& p) {
     for (int n = 0; n < p.N; ++n) {
         const size_t fb = (size_t)p.dims[n] * p.Rp * sizeof(float);

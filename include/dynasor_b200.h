@@ -232,6 +232,33 @@ int dgpu_plan_set_timing(dgpu_plan* plan, int enable);
 int dgpu_plan_get_timing(dgpu_plan* plan, dgpu_kernel_timing* out, int max,
                          int* count, int reset);
 
+/* ---- autotuning (no single reference counterpart: the reference fixes its
+ *      chunking at compile time; pick_mn, src/dynasor_preprocess.cpp:87-99,
+ *      chooses only the rows per shard, and the plan keeps that choice) -----
+ * Picks the plan's partition chunk sizes, LSD digit widths and MTTKRP grid
+ * target by timing whole sweeps: coordinate descent over
+ *   fiber_digit_bits {5,6,7,8}, sort_digit_bits {6,7,8}, chunks_per_sm
+ *   {2,4,8}, seg_chunk_tiles {4,8,16} (PingPong plans; the fiber knobs only
+ *   with fiber-sorted modes) and mttkrp_ctas_per_sm {2,4,8} (all layouts),
+ * one warm-up and `sweeps` (1..50) timed sweeps per candidate, the fastest
+ * kept.  No knob changes a slab permutation, and results change only by
+ * FP32 summation order.  A PingPong plan must be between sweeps
+ * (DGPU_ERR_ORDER otherwise); the sweeps it times advance its slab as any
+ * sweep does (to the reference's slab after that many more sweeps), so tune
+ * before work whose slab order matters.  Cached CP-ALS graphs of the plan
+ * are recaptured afterwards.  Morton plans give DGPU_ERR_ARG.  Synchronises. */
+typedef struct {
+    int       fiber_digit_bits;      /* bits per LSD pass of the fiber sort */
+    int       sort_digit_bits;       /* bits per LSD pass of the remap      */
+    int       chunks_per_sm;         /* remap partition chunks per SM       */
+    int       seg_chunk_tiles;       /* fiber partition: 4096-nnz tiles per chunk */
+    int       mttkrp_ctas_per_sm;    /* MTTKRP tile split target            */
+    int       candidates;            /* configurations timed                */
+    double    default_ms;            /* ms per sweep before tuning          */
+    double    tuned_ms;              /* ms per sweep with the chosen values */
+} dgpu_tune_result;
+int dgpu_plan_autotune(dgpu_plan* plan, int sweeps, dgpu_tune_result* out);
+
 /* Plan tables (src/dynasor_preprocess.cpp:291-463): shard ranges of mode n
  * (K entries each), and the LPT schedule as per-worker counts plus the
  * concatenated shard lists.  *n_listed receives the number of shards. */
