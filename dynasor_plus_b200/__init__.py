@@ -442,6 +442,15 @@ class Plan:
         return out
 
 
+def init_factor(seed: int, n: int, rows: int, rank: int):
+    """The reference's seeded N(0,1) initial factor of mode n (host only):
+    rows x Rp float32, padding zero -- what cpals starts from."""
+    Rp = padded_rank(rank)
+    Y = np.zeros((int(rows), Rp), np.float32)
+    check(lib().dgpu_init_factor(int(seed), int(n), int(rows), int(rank), Rp, Y.ctypes.data))
+    return Y
+
+
 def spmttkrp_dynasor(plan: Plan, Y):
     """One all-modes sweep from host factors; returns (Yhat list, seconds).
     Mirrors spmttkrp_dynasor (src/dynasor.cpp:545-559)."""

@@ -132,6 +132,7 @@ _SIGS = {
     "dgpu_download_copy": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "dgpu_cp_options_default": (None, [C.POINTER(CpOptions)]),
     "dgpu_cpals": (C.c_int, [C.c_void_p, C.POINTER(CpOptions), C.POINTER(CpResult), C.c_void_p]),
+    "dgpu_init_factor": (C.c_int, [C.c_uint64, C.c_int, C.c_uint32, C.c_int, C.c_int, C.c_void_p]),
     "dgpu_cpals_multistart": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CpOptions), C.c_void_p,
                                         C.c_void_p]),
     "dgpu_cpals_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CpOptions), C.c_void_p,

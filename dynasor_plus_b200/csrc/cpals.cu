@@ -1046,6 +1046,20 @@ int update_mode(Plan& p, const LaLayout& L, int n, int solve_fp64, double ridge,
 // from the other modes' Grams, and its Gram is recomputed from the result),
 // so a Gauss-Seidel run skips the draw of mode 0 -- on the 1M-row rank-32
 // factor, 32M normal draws.
+// One mode's factor (rows x Rp, row-major, padding zero) into host memory.
+void draw_factor(uint64_t seed, int n, uint32_t rows, int R, int Rp, float* y) {
+    uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
+    z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
+    z ^= z >> 27; z *= 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    std::mt19937_64 rng(z);
+    std::normal_distribution<float> g(0.0f, 1.0f);
+    for (uint32_t i = 0; i < rows; ++i) {
+        for (int r = 0; r < R; ++r) y[(size_t)i * Rp + r] = g(rng);
+        for (int r = R; r < Rp; ++r) y[(size_t)i * Rp + r] = 0.f;
+    }
+}
+
 int init_factors_host(Plan& p, uint64_t seed, int skip_mode) {
     // one independent generator per mode: draw the modes on parallel host
     // threads (large factors take seconds to draw serially)
@@ -1057,15 +1071,8 @@ int init_factors_host(Plan& p, uint64_t seed, int skip_mode) {
     for (int n = 0; n < p.N; ++n) {
         if (n == skip_mode) continue;
         auto draw = [&, n]() {
-            uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (uint64_t)(n + 1);
-            z ^= z >> 30; z *= 0xBF58476D1CE4E5B9ULL;
-            z ^= z >> 27; z *= 0x94D049BB133111EBULL;
-            z ^= z >> 31;
-            std::mt19937_64 rng(z);
-            std::normal_distribution<float> g(0.0f, 1.0f);
             Y[n].assign((size_t)p.dims[n] * p.Rp, 0.f);
-            for (uint32_t i = 0; i < p.dims[n]; ++i)
-                for (int r = 0; r < p.R; ++r) Y[n][(size_t)i * p.Rp + r] = g(rng);
+            draw_factor(seed, n, p.dims[n], p.R, p.Rp, Y[n].data());
         };
         if (par) th.emplace_back(draw);
         else draw();
@@ -1794,6 +1801,18 @@ int cpopt_gradient(Plan& p, float* const* grad_host) {
 }
 
 }  // namespace dgpu
+
+// The reference's initial factor of mode n (init_random_factors,
+// src/dynasor_cpals.cpp:42-69) into host memory: no device involved.
+extern "C" int dgpu_init_factor(uint64_t seed, int n, uint32_t rows, int R, int Rp, float* Y) {
+    using namespace dgpu;
+    if (!Y || n < 0 || n >= kMaxModes || R < 1 || Rp < R) {
+        set_error("dgpu_init_factor: bad argument");
+        return DGPU_ERR_ARG;
+    }
+    draw_factor(seed, n, rows, R, Rp, Y);
+    return DGPU_OK;
+}
 
 // Standalone Gram G = Y^T Y (R x R, leading dimension R) of a device matrix
 // (replaces la::gram, src/dynasor_linalg.cpp:47-99).  Temporary partials

@@ -316,6 +316,11 @@ void dgpu_cp_options_default(dgpu_cp_options* opt);
 int  dgpu_cpals(dgpu_plan* plan, const dgpu_cp_options* opt,
                 dgpu_cp_result* res, double* fit_history);
 
+/* The reference's seeded N(0,1) initial factor of mode n (init_random_factors,
+ * src/dynasor_cpals.cpp:42-69): rows x Rp row-major host buffer, padding
+ * zero; the draws dgpu_cpals starts from.  Host only, no device needed. */
+int  dgpu_init_factor(uint64_t seed, int n, uint32_t rows, int R, int Rp, float* Y);
+
 /* K random-restart CP-ALS runs in one plan (no single reference function:
  * the reference runs cpals, src/dynasor_cpals.cpp:120-396, once per seed).
  * The plan's rank is restarts * Re (Re <= 64); restart k uses columns
