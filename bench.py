@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--cpals-iters", type=int, default=5)
     ap.add_argument("--no-bf16", action="store_true",
                     help="skip the BF16-gather CP-ALS block (4-mode rank-64 tensor)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched blocks (16 restarts; 32 tensors)")
     ap.add_argument("--json-out", default=None)
     return ap.parse_args()
 
@@ -220,6 +222,70 @@ def bf16_block(device, stream, args):
                        "fp32_final_fit": f32["final_fit"], "bf16_final_fit": b16["final_fit"],
                        "max_abs_fit_diff_bf16_vs_fp32": float(np.max(np.abs(
                            b16["fit_history"] - f32["fit_history"])))}
+    return out
+
+
+def batched_block(device, stream, args):
+    """The two batched CP-ALS workloads, each against the same runs one by
+    one (Gauss-Seidel, FP64 solve, NCopy layout; the second call of each is
+    timed, after a first call on the same plans):
+      * 16 random restarts of rank 16 on 400,000 x 300,000 x 2,000 from 50M
+        Zipf(1.0) draws, rank-8 |N(0,1)| truth + 2% noise: one plan of rank
+        256 (dgpu_cpals_multistart) vs 16 plans of rank 16, 10 iterations;
+      * 32 tensors, dims log-uniform in [1e3, 1e5], nnz log-uniform in
+        [1e4, 5e6], rank-4 truth + 1% noise, rank 8, 30 iterations, tol 1e-4:
+        dgpu_cpals_batch vs dgpu_cpals per tensor."""
+    import torch
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    out = {}
+    dims, vals, idx = synth.cp_zipf_torch((400_000, 300_000, 2_000), 50_000_000, (1.0, 1.0, 1.0),
+                                          8, 0.02, 4, "cuda")
+    K, Re, it = 16, 16, 10
+    p = d.Plan(dims, vals, idx, threads=args.threads, rank=K * Re, layout="ncopy", device=device)
+    p.set_stream(stream)
+    p.cpals_multistart(K, max_iters=it, tol=0.0, seed=42)
+    t0 = time.time()
+    p.cpals_multistart(K, max_iters=it, tol=0.0, seed=42)
+    tb = time.time() - t0
+    p.close()
+    single = []
+    for k in range(K):
+        q = d.Plan(dims, vals, idx, threads=args.threads, rank=Re, layout="ncopy", device=device)
+        q.set_stream(stream)
+        q.cpals(max_iters=it, tol=0.0, seed=42 + k)
+        t0 = time.time()
+        q.cpals(max_iters=it, tol=0.0, seed=42 + k)
+        single.append(time.time() - t0)
+        q.close()
+    out["restarts"] = {"workload": f"400000x300000x2000, {len(vals)} nnz, {K} restarts x rank {Re}, "
+                                   f"{it} iterations", "batched_s": tb, "one_by_one_s": sum(single),
+                       "speedup": sum(single) / tb}
+    del dims, vals, idx
+    ts = synth.tensor_batch(32, seed=17)
+    plans = [d.Plan(dm, v, i, threads=args.threads, rank=8, layout="ncopy", device=device)
+             for dm, v, i in ts]
+    t0 = time.time()
+    d.cpals_batch(plans, max_iters=30, tol=1e-4, seed=42)
+    cold = time.time() - t0
+    t0 = time.time()
+    d.cpals_batch(plans, max_iters=30, tol=1e-4, seed=42)
+    tb = time.time() - t0
+    one, one_cold = 0.0, 0.0
+    for pl in plans:
+        t0 = time.time()
+        pl.cpals(max_iters=30, tol=1e-4, seed=42)
+        one_cold += time.time() - t0
+        t0 = time.time()
+        pl.cpals(max_iters=30, tol=1e-4, seed=42)
+        one += time.time() - t0
+    for pl in plans:
+        pl.close()
+    out["tensors"] = {"workload": f"32 tensors, {sum(len(v) for _, v, _ in ts)} nnz in all, rank 8, "
+                                  "30 iterations, tol 1e-4",
+                      "batched_s": tb, "one_by_one_s": one, "speedup": one / tb,
+                      "first_call_batched_s": cold, "first_call_one_by_one_s": one_cold}
+    torch.cuda.synchronize()
     return out
 
 
@@ -536,6 +602,11 @@ def main():
             out["bf16"] = bf16_block(local, stream, args)
         except Exception as ex:  # reported, never required
             out["bf16"] = {"error": str(ex)[:300]}
+    if rank == 0 and not args.no_batched and args.cpals_iters > 0:
+        try:
+            out["batched"] = batched_block(local, stream, args)
+        except Exception as ex:  # reported, never required
+            out["batched"] = {"error": str(ex)[:300]}
     if rank == 0:
         s = json.dumps(out)
         print(s)
