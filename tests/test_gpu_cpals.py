@@ -181,11 +181,15 @@ def test_four_mode_bf16_rank64_against_fp64_oracle(bindings, kernel):
           + " ".join(f"{e:.2e}" for e in e64) + "; vs BF16-rounded FP64 "
           + " ".join(f"{e:.2e}" for e in eb))
     # BF16 rounding of the gathered factors moves the factors by ~5e-3
-    # (GS, 3 iterations) and ~7e-3 (Jacobi, 2) against FP64, the fit by
-    # < 1e-6; the same rounding in FP64 leaves only FP32 accumulation
+    # (GS, 3 iterations) and ~4e-3 (Jacobi, 2) against FP64, the fit by
+    # < 1e-6.  Against the same rounding in FP64 only FP32 accumulation is
+    # left, but from the second iteration on an FP32-level difference can
+    # flip the BF16 rounding of a gathered entry (a 2^-9 relative step):
+    # measured 1.9e-4 (GS) and 1.5e-5 (Jacobi); one iteration on the
+    # 200M-nonzero tensor stays within 2e-5 (tests/test_gpu_configs.py)
     assert df < FIT_TOL
     assert max(e64) < 1.5e-2
-    assert max(eb) < 1e-4
+    assert max(eb) < 1e-3
     p.close()
 
 
