@@ -159,24 +159,22 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     uint32_t cur = 0xffffffffu;
     bool first_run = true;                 // the run at the start of this group's slice
 
-    // U == 1: the gathered rows stay in registers from one nonzero to the
-    // next, and a row is loaded only when its index differs from the
-    // previous nonzero's.  Inside a fiber-sorted row run of mode n the
-    // nonzeros keep the previous mode's processing order, which is sorted by
-    // that mode's index, so equal (i_n, i_{n-1}) pairs are consecutive: on
-    // the 3-mode Zipf(1.1) tensor 56-68% of one of the two gathers repeat
-    // the previous nonzero's row.  The arithmetic is unchanged (same values,
-    // same order); only the load is skipped.
-    float yk[N][V][4];
-    uint32_t last[N];
+    // U == 1: the previous mode's gathered row stays in registers from one
+    // nonzero to the next and is loaded again only when its index changes.
+    // Inside a fiber-sorted row run of mode n the nonzeros keep mode n-1's
+    // processing order, which is sorted by mode n-1's index, so equal
+    // (i_n, i_{n-1}) pairs are consecutive: on the 3-mode Zipf(1.1) tensor
+    // 56-68% of mode n-1's row gathers repeat the previous nonzero's row.
+    // Only that one row is kept (the other modes' indices rarely repeat
+    // back to back), which adds 4 registers per V, not 4 per gathered mode.
+    // The arithmetic is unchanged (same values, same order).
+    const int wp = (n + N - 1) % N;
+    float yp[V][4];
+    uint32_t lastp = 0xffffffffu;
 #pragma unroll
-    for (int w = 0; w < N; ++w) {
-        last[w] = 0xffffffffu;
+    for (int v = 0; v < V; ++v)
 #pragma unroll
-        for (int v = 0; v < V; ++v)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) yk[w][v][q] = 0.f;
-    }
+        for (int q = 0; q < 4; ++q) yp[v][q] = 0.f;
 
     // prefetch registers for one chunk
     uint32_t pf[LPE][SW];
@@ -227,23 +225,23 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
 #pragma unroll
                 for (int w = 0; w < N; ++w) {
                     const uint32_t id = s[1 + w];
-                    if constexpr (U == 1) {
-                        if (w != n && id != last[w]) {
-                            last[w] = id;
+                    if (U == 1 && w == wp) {
+                        if (id != lastp) {
+                            lastp = id;
 #pragma unroll
                             for (int v = 0; v < V; ++v) {
                                 const int c4 = gl + v * G;
                                 if (V == 1 || c4 < C4) {
                                     const float4 g4 = gather4<BF>(F, w, id, ld, c4);
-                                    yk[w][v][0] = g4.x; yk[w][v][1] = g4.y;
-                                    yk[w][v][2] = g4.z; yk[w][v][3] = g4.w;
+                                    yp[v][0] = g4.x; yp[v][1] = g4.y;
+                                    yp[v][2] = g4.z; yp[v][3] = g4.w;
                                 }
                             }
                         }
 #pragma unroll
                         for (int v = 0; v < V; ++v)
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) y[u][w][v][q] = yk[w][v][q];
+                            for (int q = 0; q < 4; ++q) y[u][w][v][q] = yp[v][q];
                     } else {
 #pragma unroll
                         for (int v = 0; v < V; ++v) {
