@@ -1388,6 +1388,18 @@ struct CpSession {
         st_bytes = need;
         return DGPU_OK;
     }
+    // BF16 mirrors of every factor changed since its last conversion.  A
+    // loop graph converts, per mode, the mirrors that were stale when it was
+    // captured (the steady state of the capturing run: the factors updated
+    // since the previous mode), so a graph kept from an earlier run assumes
+    // the other mirrors current.  Fresh initial factors leave them stale:
+    // convert them before such a graph runs.
+    int refresh_mirrors() {
+        if (p.precision != DGPU_PREC_BF16) return DGPU_OK;
+        for (int n = 0; n < p.N; ++n)
+            if (p.yb_stale[n]) DGPU_TRY(launch_to_bf16(p, n));
+        return DGPU_OK;
+    }
     int write_state() {
         const double init[2] = {(double)it, fit_prev};
         DGPU_CUDA(cudaMemcpyAsync(st, init, sizeof(init), cudaMemcpyHostToDevice, p.stream));
@@ -1591,6 +1603,7 @@ int run_loop_cached(CpSession& s) {
         }
         std::memcpy(p.cp_loop_key, key, sizeof(key));
     } else {
+        DGPU_TRY(s.refresh_mirrors());
         DGPU_TRY(s.write_state());
     }
     DGPU_CUDA(cudaEventRecord(s.ev[0], p.stream));
@@ -1679,7 +1692,10 @@ int cpals_batch_run(Plan* const* plans, int count, const dgpu_cp_options& o,
         cached = owner.cp_batch_exec != nullptr && batch_key(all) == owner.cp_batch_key;
     }
     if (cached) {
-        for (CpSession* s : all) DGPU_TRY(s->write_state());
+        for (CpSession* s : all) {
+            DGPU_TRY(s->refresh_mirrors());
+            DGPU_TRY(s->write_state());
+        }
         DGPU_TRY(launch_loops(all, owner.cp_batch_exec, owner.stream));
     } else {
         for (CpSession* s : all)

@@ -159,23 +159,6 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     uint32_t cur = 0xffffffffu;
     bool first_run = true;                 // the run at the start of this group's slice
 
-    // U == 1: the previous mode's gathered row stays in registers from one
-    // nonzero to the next and is loaded again only when its index changes.
-    // Inside a fiber-sorted row run of mode n the nonzeros keep mode n-1's
-    // processing order, which is sorted by mode n-1's index, so equal
-    // (i_n, i_{n-1}) pairs are consecutive: on the 3-mode Zipf(1.1) tensor
-    // 56-68% of mode n-1's row gathers repeat the previous nonzero's row.
-    // Only that one row is kept (the other modes' indices rarely repeat
-    // back to back), which adds 4 registers per V, not 4 per gathered mode.
-    // The arithmetic is unchanged (same values, same order).
-    const int wp = (n + N - 1) % N;
-    float yp[V][4];
-    uint32_t lastp = 0xffffffffu;
-#pragma unroll
-    for (int v = 0; v < V; ++v)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) yp[v][q] = 0.f;
-
     // prefetch registers for one chunk
     uint32_t pf[LPE][SW];
     auto prefetch = [&](uint32_t ch) {
@@ -225,32 +208,13 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
 #pragma unroll
                 for (int w = 0; w < N; ++w) {
                     const uint32_t id = s[1 + w];
-                    if (U == 1 && w == wp) {
-                        if (id != lastp) {
-                            lastp = id;
 #pragma unroll
-                            for (int v = 0; v < V; ++v) {
-                                const int c4 = gl + v * G;
-                                if (V == 1 || c4 < C4) {
-                                    const float4 g4 = gather4<BF>(F, w, id, ld, c4);
-                                    yp[v][0] = g4.x; yp[v][1] = g4.y;
-                                    yp[v][2] = g4.z; yp[v][3] = g4.w;
-                                }
-                            }
-                        }
-#pragma unroll
-                        for (int v = 0; v < V; ++v)
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) y[u][w][v][q] = yp[v][q];
-                    } else {
-#pragma unroll
-                        for (int v = 0; v < V; ++v) {
-                            const int c4 = gl + v * G;
-                            float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                            if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
-                            y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
-                            y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
-                        }
+                    for (int v = 0; v < V; ++v) {
+                        const int c4 = gl + v * G;
+                        float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
+                        y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
+                        y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
                     }
                 }
             }

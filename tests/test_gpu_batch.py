@@ -46,19 +46,21 @@ def test_batch_rejects_repeated_plan():
     p.close()
 
 
-@pytest.mark.parametrize("layout", ["ncopy", "pingpong"])
-def test_repeated_batch_reuses_its_loop_graph(layout):
+@pytest.mark.parametrize("layout,precision", [("ncopy", "fp32"), ("pingpong", "fp32"),
+                                              ("ncopy", "bf16")])
+def test_repeated_batch_reuses_its_loop_graph(layout, precision):
     """The batch's loop graph is kept on its first plan: a second call with
     the same options runs every iteration, the first included, in it; a call
     with other options captures a new one; every call equals single runs."""
     import dynasor_plus_b200 as d
     ts = _tensors()
-    plans = [d.Plan(dims, v, i, threads=8, rank=8, layout=layout) for dims, v, i in ts]
+    plans = [d.Plan(dims, v, i, threads=8, rank=8, layout=layout, precision=precision)
+             for dims, v, i in ts]
     want = {}
     for tol in (1e-4, 1e-3):
         want[tol] = []
         for dims, v, i in ts:
-            q = d.Plan(dims, v, i, threads=8, rank=8, layout=layout)
+            q = d.Plan(dims, v, i, threads=8, rank=8, layout=layout, precision=precision)
             want[tol].append(q.cpals(max_iters=40, tol=tol, seed=42))
             q.close()
     for tol in (1e-4, 1e-4, 1e-3, 1e-4, 1e-4):

@@ -193,22 +193,24 @@ def test_four_mode_bf16_rank64_against_fp64_oracle(bindings, kernel):
     p.close()
 
 
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
 @pytest.mark.parametrize("layout", ["pingpong", "ncopy"])
-def test_repeated_runs_reuse_the_device_loop(layout):
+def test_repeated_runs_reuse_the_device_loop(layout, precision):
     """The device-loop graph is kept on the plan: a second run with the
     same options relaunches it, a run with other options captures a new one,
     and every run gives the fit trajectory of an eager run (graphs off) from
-    the same seed."""
+    the same seed.  With BF16 gathers the relaunched graph must start from
+    mirrors of the new run's initial factors, not the last run's."""
     import dynasor_plus_b200 as d
     g = load_golden("ref_cpals_r5.npz")
     dims = g["dims"]
     idx = [g[f"idx{n}"] for n in range(len(dims))]
     T, R = int(g["T"]), int(g["R"])
-    e = d.Plan(dims, g["vals"], idx, threads=T, rank=R, layout=layout)
+    e = d.Plan(dims, g["vals"], idx, threads=T, rank=R, layout=layout, precision=precision)
     want = {tol: e.cpals(max_iters=20, tol=tol, seed=42, graphs=False)["fit_history"]
             for tol in (0.0, 1e-3)}
     e.close()
-    p = d.Plan(dims, g["vals"], idx, threads=T, rank=R, layout=layout)
+    p = d.Plan(dims, g["vals"], idx, threads=T, rank=R, layout=layout, precision=precision)
     for tol in (0.0, 0.0, 1e-3, 0.0, 1e-3, 1e-3):
         r = p.cpals(max_iters=20, tol=tol, seed=42)
         h = r["fit_history"]
