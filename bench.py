@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--cpals-iters", type=int, default=5)
     ap.add_argument("--no-bf16", action="store_true",
                     help="skip the BF16-gather CP-ALS block (4-mode rank-64 tensor)")
+    ap.add_argument("--bf16-draws", type=int, default=200_000_000,
+                    help="coordinate draws of the 4-mode tensor of the BF16 block")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched blocks (16 restarts; 32 tensors)")
     ap.add_argument("--json-out", default=None)
@@ -199,11 +201,11 @@ def bf16_block(device, stream, args):
     import torch
     import dynasor_plus_b200 as d
     from dynasor_plus_b200 import synth
-    dims, vals, idx = synth.cp_zipf_torch((50_000, 20_000, 2_000, 500), 200_000_000,
+    dims, vals, idx = synth.cp_zipf_torch((50_000, 20_000, 2_000, 500), args.bf16_draws,
                                           (0, 0, 1.3, 1.3), 10, 0.05, 3, "cuda")
     it = args.cpals_iters
-    out = {"workload": f"4-mode 50000x20000x2000x500, 200M draws deduped to {len(vals)} nnz, "
-                       "rank 64, GS, FP64 solve", "iters": it}
+    out = {"workload": f"4-mode 50000x20000x2000x500, {args.bf16_draws} draws deduped to "
+                       f"{len(vals)} nnz, rank 64, GS, FP64 solve", "iters": it}
     for layout in ("ncopy", "pingpong"):
         res = {}
         for prec in ("fp32", "bf16"):
