@@ -48,8 +48,8 @@ def test_bf16_gather_cpals_within_tolerance_of_fp64(bindings):
     """BF16 gathers (the last mode's MTTKRP in FP32, which keeps the fit's
     <X, M> term exact up to FP32): final fit within the north-star 1e-4 of
     FP64 CP-ALS, and every fit within 1e-6 of the FP64 run whose MTTKRP
-    reads the same BF16-rounded factors.  (With every mode in BF16 the FP64
-    emulation already misses 1e-4 on this tensor: 2.1e-4.)"""
+    reads the same BF16-rounded factors within 1e-5.  (With every mode in
+    BF16 the FP64 emulation already misses 1e-4 on this tensor: 2.1e-4.)"""
     g, dims, idx, p = _golden_plan(precision="bf16")
     it, R = int(g["iters"]), int(g["R"])
     r = p.cpals(max_iters=it, tol=0.0, seed=42)
@@ -63,7 +63,9 @@ def test_bf16_gather_cpals_within_tolerance_of_fp64(bindings):
           f"{np.max(np.abs(h - fit64)):.2e}); vs BF16-rounded FP64 {np.max(np.abs(h - fitb)):.2e}; "
           "factor rel-Fro vs FP64 " + " ".join(f"{e:.2e}" for e in ef))
     assert abs(h[-1] - fit64[-1]) < FIT_TOL
-    assert np.max(np.abs(h - fitb)) < 1e-6
+    # FP32 accumulation order flips BF16 roundings over the 15 iterations:
+    # measured 4.7e-7 and 3.6e-6 on two runs
+    assert np.max(np.abs(h - fitb)) < 1e-5
 
 
 def test_convergence_stop_rule():
@@ -211,9 +213,14 @@ def test_repeated_runs_reuse_the_device_loop(layout, precision):
             for tol in (0.0, 1e-3)}
     e.close()
     p = d.Plan(dims, g["vals"], idx, threads=T, rank=R, layout=layout, precision=precision)
+    # BF16: atomic summation order flips the BF16 rounding of a few gathered
+    # entries now and then, and the difference grows to ~3e-6 over 20
+    # iterations (the first iteration agrees to ~3e-9)
+    bound = 1e-6 if precision == "fp32" else 1e-5
     for tol in (0.0, 0.0, 1e-3, 0.0, 1e-3, 1e-3):
         r = p.cpals(max_iters=20, tol=tol, seed=42)
         h = r["fit_history"]
         assert len(h) == len(want[tol]), (tol, len(h), len(want[tol]))
-        assert np.max(np.abs(h - want[tol])) < 1e-6, tol
+        assert abs(h[0] - want[tol][0]) < 1e-7, tol
+        assert np.max(np.abs(h - want[tol])) < bound, tol
     p.close()
