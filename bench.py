@@ -47,15 +47,16 @@ SEED = 2
 RANK = 32
 METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per nonzero per
-# launch, from one ncu capture of the same kernels on the 20M-draw case of
-# this workload (14,569,916 nnz; profiles/traffic_zipf1.1_14.6M.md).  Both
-# kernels stream the slab once per launch, so their traffic grows with nnz;
-# the bench scales these figures to its own nnz for `roofline.traffic`.
-NCU_DRAM_BYTES_PER_NNZ = {
-    "part_scatter": 29.35,     # k_chunk_scatter, all launches averaged
-    "fiber_scatter": 29.35,
-    "mttkrp": 47.01,           # k_mttkrp_rowrun, 3 modes averaged
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch,
+# measured by ncu on this workload at its full size (64,659,576 nnz, the
+# timed sweep of `bench.py --steps 1 --warmup 1`; one-pass metrics):
+# profiles/dram_traffic_zipf1.1_64.7M.md.  Averages over the sweep's launches
+# of each kind; scaled by nnz only when the bench runs another size.
+NCU_NNZ = 64_659_576
+NCU_DRAM_BYTES_PER_LAUNCH = {
+    "part_scatter": 2_117_256_619,     # k_chunk_scatter, the 3 remap passes
+    "fiber_scatter": 2_152_501_589,    # k_chunk_scatter, the 6 fiber-sort passes
+    "mttkrp": 3_014_740_139,           # k_mttkrp_rowrun, 3 modes (2.38 / 3.19 / 3.48 GB)
 }
 
 
@@ -524,15 +525,20 @@ def main():
                            "peak_source": peak_src},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (NCU_DRAM_BYTES_PER_NNZ[dom] * nnz
-                                 if dom in NCU_DRAM_BYTES_PER_NNZ else None),
-                     "traffic_source": "ncu dram bytes per nnz on the 14.6M-nnz case, scaled",
+                     "traffic": (NCU_DRAM_BYTES_PER_LAUNCH[dom] * nnz / NCU_NNZ
+                                 if dom in NCU_DRAM_BYTES_PER_LAUNCH else None),
+                     "traffic_source": ("ncu dram bytes per launch at this size" if nnz == NCU_NNZ
+                                        else "ncu dram bytes per launch at 64,659,576 nnz, "
+                                             "scaled by nnz"),
                      "peak_source": peak_src, "avg_launch_ms": dom_ms,
                      "algorithmic_bytes_per_launch": dom_bytes},
         "kernel_rooflines": {
             k: {"achieved_gbs": (v["bytes"] / v["launches"]) / (v["total_ms"] / v["launches"] * 1e-3) / 1e9,
                 "frac": (v["bytes"] / v["launches"]) / (v["total_ms"] / v["launches"] * 1e-3) / 1e9 / peak,
-                "avg_launch_ms": v["total_ms"] / v["launches"]}
+                "avg_launch_ms": v["total_ms"] / v["launches"],
+                "algorithmic_bytes_per_launch": v["bytes"] / v["launches"],
+                "traffic_per_launch": (NCU_DRAM_BYTES_PER_LAUNCH[k] * nnz / NCU_NNZ
+                                       if k in NCU_DRAM_BYTES_PER_LAUNCH else None)}
             for k, v in tim.items() if v["launches"] and v["total_ms"] > 0},
         "kernel_times_ms_per_step": {k: v["total_ms"] / 2 for k, v in tim.items() if v["launches"]},
         "kernel_share": {k: v["total_ms"] / total_ms for k, v in tim.items() if v["launches"]},
