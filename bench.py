@@ -83,6 +83,8 @@ def parse():
                     help="skip the BF16-gather CP-ALS block (4-mode rank-64 tensor)")
     ap.add_argument("--bf16-draws", type=int, default=200_000_000,
                     help="coordinate draws of the 4-mode tensor of the BF16 block")
+    ap.add_argument("--no-cpopt", action="store_true",
+                    help="skip the CP-OPT forward / gradient block (20M-nonzero tensor)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched blocks (16 restarts; 32 tensors)")
     ap.add_argument("--json-out", default=None)
@@ -289,6 +291,40 @@ def batched_block(device, stream, args):
                       "batched_s": tb, "one_by_one_s": one, "speedup": one / tb,
                       "first_call_batched_s": cold, "first_call_one_by_one_s": one_cold}
     torch.cuda.synchronize()
+    return out
+
+
+def cpopt_block(device, stream, args):
+    """CP-OPT forward (model values at the nonzeros, FP32, to a host buffer)
+    and gradient (every factor's, to host buffers) on 100,000 x 100,000 x
+    1,000 with 20M uniform nonzeros, N(0,1) values, rank 32, factors
+    N(0, 0.1); NCopy and PingPong plans; 3 timed calls after one warm-up."""
+    import torch
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.uniform((100_000, 100_000, 1_000), 20_000_000, seed=21, values="normal")
+    rng = np.random.default_rng(22)
+    Y = [np.asarray(rng.normal(0, 0.1, (int(n), 32)), np.float32) for n in dims]
+    out = {"workload": "100000x100000x1000, 20M uniform nnz, rank 32", "nnz": len(vals)}
+    for layout in ("ncopy", "pingpong"):
+        p = d.Plan(dims, vals, idx, threads=args.threads, rank=32, layout=layout, device=device)
+        p.set_stream(stream)
+        for n in range(3):
+            p.set_factor(n, Y[n])
+        p.model_values()
+        p.cpopt_gradient()
+        torch.cuda.synchronize()
+        t0 = time.time()
+        for _ in range(3):
+            p.model_values()
+        tf = (time.time() - t0) / 3
+        t0 = time.time()
+        for _ in range(3):
+            p.cpopt_gradient()
+        tg = (time.time() - t0) / 3
+        out[layout] = {"forward_ms": tf * 1e3, "forward_gnnz_s": len(vals) / tf / 1e9,
+                       "gradient_ms": tg * 1e3, "gradient_gnnz_s": len(vals) / tg / 1e9}
+        p.close()
     return out
 
 
@@ -610,6 +646,11 @@ def main():
             out["bf16"] = bf16_block(local, stream, args)
         except Exception as ex:  # reported, never required
             out["bf16"] = {"error": str(ex)[:300]}
+    if rank == 0 and not args.no_cpopt and args.cpals_iters > 0:
+        try:
+            out["cpopt"] = cpopt_block(local, stream, args)
+        except Exception as ex:  # reported, never required
+            out["cpopt"] = {"error": str(ex)[:300]}
     if rank == 0 and not args.no_batched and args.cpals_iters > 0:
         try:
             out["batched"] = batched_block(local, stream, args)
