@@ -23,7 +23,18 @@ time, scaling "weak".
 
 --impl reference times the reference's own CPU implementation (the
 reference sources compiled into oracle/_ref) on this host's cores, on the
-same workload and metric.
+same workload and metric: one PingPong sweep of the whole tensor per step.
+`cpu_baseline` is the same reference on the whole tensor, median of
+--cpu-sweeps sweeps.
+
+Beside the headline the line carries, each measured on its own workload:
+`cpals` / `cpals_small` (CP-ALS iterations/s on this tensor and on the
+200^3 / 100k-nonzero rank-16 configuration), `ncopy` (the NCopy layout),
+`bf16` (4-mode 50,000 x 20,000 x 2,000 x 500 from 200M draws, rank 64:
+CP-ALS iterations/s with FP32 and with BF16 gathers), `cpopt` (forward and
+gradient on 100,000 x 100,000 x 1,000 with 20M nonzeros, rank 32) and
+`batched` (16 restarts of rank 16 in one plan; 32 tensors in one batch;
+each against the same runs one by one).
 """
 from __future__ import annotations
 
