@@ -212,6 +212,10 @@ struct Plan {
     int          chunks_per_sm = 4;             // global (remap) partition: chunks per SM
     int          seg_chunk_tiles = 16;          // segmented (fiber) partition: tiles per chunk
     int          mttkrp_ctas_per_sm = 4;        // tiles are split until this many CTAs per SM
+    // MTTKRP gathers: 0 per-lane loads (mttkrp.cu, any shape), 1 the TMA
+    // engine's tile::gather4 into a shared-memory ring (mttkrp_tma.cu;
+    // 3 and 4 modes, Rp 16/32/64, whole rows)
+    int          mttkrp_kernel = 0;
     float*       Y[kMaxModes] = {nullptr};
     float*       Yhat[kMaxModes] = {nullptr};
     __nv_bfloat16* Yb[kMaxModes] = {nullptr};
@@ -393,6 +397,12 @@ int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t nt
 int launch_mttkrp_all_modes(Plan& p);
 // Values array of the live nonzeros (any order).
 const float* live_vals(const Plan& p);
+
+// MTTKRP with TMA row gathers (mttkrp_tma.cu): whether the plan's shape has
+// a variant for `cols` columns per pass, and the launch.
+bool gather_supported(const Plan& p, int cols);
+int launch_mttkrp_gather(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
+                         bool bf, int wl, int rows_contiguous);
 
 // FP32 -> BF16 factor mirror.
 int launch_to_bf16(Plan& p, int n);

@@ -517,6 +517,9 @@ int launch_n(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles,
 {
     if (mttkrp_scheme(p, n) == DGPU_ACCUM_PRIVATE)
         return launch_priv<N, BF>(p, n, in, tiles, ntiles, F, w0, wl);
+    if (p.mttkrp_kernel == 1 && gather_supported(p, p.Rp))
+        return launch_mttkrp_gather(p, n, in, tiles, ntiles, BF, wl,
+                                    (p.fiber && p.kclass[n] == 2) ? 1 : 0);
     // Rank tiles: one pass over the slab per tile of `rt` columns.  Wide
     // factors gather whole rows per nonzero, which spills the hot rows out
     // of L1; narrower tiles re-read the slab but keep gathers cached.  The

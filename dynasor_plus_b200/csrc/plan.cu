@@ -397,6 +397,7 @@ static int plan_init(Plan& p, int N, uint64_t nnz, const uint32_t* dims, const d
     // does not depend on them)
     if (const char* e = std::getenv("DGPU_SORT_DIGIT_BITS")) p.sort_digit_bits = std::atoi(e);
     if (const char* e = std::getenv("DGPU_FIBER_DIGIT_BITS")) p.fiber_digit_bits = std::atoi(e);
+    if (const char* e = std::getenv("DGPU_MTTKRP_KERNEL")) p.mttkrp_kernel = std::atoi(e) == 1 ? 1 : 0;
     if (const char* e = std::getenv("DGPU_RANK_TILE")) p.rank_tile = std::atoi(e);
     if (const char* e = std::getenv("DGPU_OVERLAP")) p.overlap = std::atoi(e);
     for (int n = 0; n < N; ++n) p.dims[n] = dims[n];

@@ -1,0 +1,56 @@
+"""The MTTKRP with TMA row gathers (mttkrp_tma.cu, DGPU_MTTKRP_KERNEL=1):
+every shape it has (3 and 4 modes, Rp 16 / 32 / 64, FP32 and BF16 rows,
+PingPong and NCopy) against FP64 (FP32 rows) or FP64 of the BF16-rounded
+factors (BF16 rows), and the remap it runs beside unchanged (the slab after
+a sweep equals the row-run kernel's plan, bit for bit)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_fro
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_round(y):
+    u = np.ascontiguousarray(y, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("layout", ["pingpong", "ncopy"])
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+@pytest.mark.parametrize("shape,draws,R", [((4000, 900, 300), 120_000, 32),
+                                            ((4000, 900, 300), 120_000, 16),
+                                            ((3000, 700, 200), 80_000, 64),
+                                            ((500, 400, 80, 30), 100_000, 64),
+                                            ((500, 400, 80, 30), 100_000, 32)])
+def test_tma_gather_mttkrp_matches_fp64(bindings, monkeypatch, layout, precision, shape, draws, R):
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.zipf(shape, draws=draws, s=1.1, seed=51)
+    N = len(dims)
+    Y = bindings.uniform_factors(8, dims, R)
+    Yr = [_bf16_round(y) for y in Y] if precision == "bf16" else Y
+    monkeypatch.setenv("DGPU_MTTKRP_KERNEL", "1")
+    p = d.Plan(dims, vals, idx, threads=4, rank=R, layout=layout, precision=precision)
+    monkeypatch.delenv("DGPU_MTTKRP_KERNEL")
+    q = d.Plan(dims, vals, idx, threads=4, rank=R, layout=layout, precision=precision)
+    for n in range(N):
+        p.set_factor(n, Y[n])
+        q.set_factor(n, Y[n])
+    for n in range(N):
+        p.process(n)
+        q.process(n)
+        y64 = bindings.mttkrp_f64(vals, idx, n, Yr, R, int(dims[n]))
+        assert rel_fro(p.yhat(n)[:, :R], y64[:, :R]) < 1e-5, n
+        assert rel_fro(p.yhat(n)[:, :R], q.yhat(n)[:, :R]) < 1e-5, n
+    pv, pi = p.slab()
+    qv, qi = q.slab()
+    assert np.array_equal(pv, qv) and all(np.array_equal(a, b) for a, b in zip(pi, qi))
+    fit = p.cpals(max_iters=3, tol=0.0, seed=42)["fit_history"]
+    fit_q = q.cpals(max_iters=3, tol=0.0, seed=42)["fit_history"]
+    assert np.max(np.abs(fit - fit_q)) < 1e-6
+    p.close()
+    q.close()
