@@ -83,7 +83,8 @@ class ComputePlan(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [("fiber_digit_bits", C.c_int), ("sort_digit_bits", C.c_int),
                 ("chunks_per_sm", C.c_int), ("seg_chunk_tiles", C.c_int),
-                ("mttkrp_ctas_per_sm", C.c_int), ("candidates", C.c_int),
+                ("mttkrp_ctas_per_sm", C.c_int), ("mttkrp_gather", C.c_int),
+                ("candidates", C.c_int),
                 ("default_ms", C.c_double), ("tuned_ms", C.c_double)]
 
 

@@ -15,6 +15,8 @@
 //    * chunks_per_sm       chunks per SM of the remap's partition
 //    * seg_chunk_tiles     4096-nonzero tiles per chunk of the fiber sort
 //    * mttkrp_ctas_per_sm  CTAs per SM the MTTKRP's tiles are split to
+//    * mttkrp_kernel       factor rows by per-lane loads or by the TMA
+//                          engine (tile::gather4), where the shape has both
 //  Coordinate descent: each knob in turn, the others held, one warm-up
 //  sweep and `sweeps` timed sweeps (CUDA events on the plan stream) per
 //  candidate, the fastest kept.  The rank tile of wide factors is tuned by
@@ -91,6 +93,7 @@ extern "C" int dgpu_plan_autotune(dgpu_plan* plan, int sweeps, dgpu_tune_result*
     if (pingpong) knobs.push_back({&p.chunks_per_sm, {2, 4, 8}, true});
     if (pingpong && any_fiber) knobs.push_back({&p.seg_chunk_tiles, {4, 8, 16}, true});
     knobs.push_back({&p.mttkrp_ctas_per_sm, {2, 4, 8}, false});
+    if (gather_supported(p, p.Rp)) knobs.push_back({&p.mttkrp_kernel, {0, 1}, false});
 
     dgpu_tune_result r{};
     double best = 0.0;
@@ -120,6 +123,7 @@ extern "C" int dgpu_plan_autotune(dgpu_plan* plan, int sweeps, dgpu_tune_result*
     r.chunks_per_sm = p.chunks_per_sm;
     r.seg_chunk_tiles = p.seg_chunk_tiles;
     r.mttkrp_ctas_per_sm = p.mttkrp_ctas_per_sm;
+    r.mttkrp_gather = p.mttkrp_kernel;
     *out = r;
     return DGPU_OK;
 }

@@ -239,7 +239,9 @@ int dgpu_plan_get_timing(dgpu_plan* plan, dgpu_kernel_timing* out, int max,
  * target by timing whole sweeps: coordinate descent over
  *   fiber_digit_bits {5,6,7,8}, sort_digit_bits {6,7,8}, chunks_per_sm
  *   {2,4,8}, seg_chunk_tiles {4,8,16} (PingPong plans; the fiber knobs only
- *   with fiber-sorted modes) and mttkrp_ctas_per_sm {2,4,8} (all layouts),
+ *   with fiber-sorted modes), mttkrp_ctas_per_sm {2,4,8} and the MTTKRP's
+ *   row gathers (per-lane loads or TMA tile::gather4, 3- and 4-mode plans of
+ *   Rp 16/32/64) (all layouts),
  * one warm-up and `sweeps` (1..50) timed sweeps per candidate, the fastest
  * kept.  No knob changes a slab permutation, and results change only by
  * FP32 summation order.  A PingPong plan must be between sweeps
@@ -253,6 +255,7 @@ typedef struct {
     int       chunks_per_sm;         /* remap partition chunks per SM       */
     int       seg_chunk_tiles;       /* fiber partition: 4096-nnz tiles per chunk */
     int       mttkrp_ctas_per_sm;    /* MTTKRP tile split target            */
+    int       mttkrp_gather;         /* 1: rows by TMA tile::gather4        */
     int       candidates;            /* configurations timed                */
     double    default_ms;            /* ms per sweep before tuning          */
     double    tuned_ms;              /* ms per sweep with the chosen values */
