@@ -1142,7 +1142,13 @@ struct CpSession {
     // host plan state saved around a capture (a capture advances it without
     // running the work)
     int cur0 = 0, nm0 = 0;
+    uint64_t pp0 = 0;
     bool stale0[kMaxModes] = {};
+    // iterations run eagerly before any capture: 2 when the first one left
+    // PingPong partition passes without kept tables (the slab's first
+    // cycle), so that the captured iterations use the kept tables
+    int warm_iters = 1;
+    bool self_map = true;                    // one iteration leaves the live slab in place
 
     CpSession(Plan& pl, const dgpu_cp_options& op, dgpu_cp_result& r, double* fh)
         : p(pl), o(op), res(r), fit_history(fh), ev(pl.cp_ev), fork(pl.cp_fork), join(pl.cp_join),
@@ -1196,11 +1202,13 @@ struct CpSession {
     void save_state() {
         cur0 = p.cur;
         nm0 = p.next_mode;
+        pp0 = p.pp_transitions;
         for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
     }
     void restore_state() {
         p.cur = cur0;
         p.next_mode = nm0;
+        p.pp_transitions = pp0;
         for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
     }
 
@@ -1292,11 +1300,11 @@ struct CpSession {
     int launch_iteration() {
         t_it = clk::now();
         const int key = (p.layout == DGPU_LAYOUT_NCOPY) ? 0 : (p.cur & 1);
-        if (graphs && it > 0 && exec[key]) {
+        if (graphs && it >= warm_iters && exec[key]) {
             DGPU_CUDA(cudaGraphLaunch(exec[key], p.stream));
             p.cur = cur_after[key];
             p.next_mode = 0;
-        } else if (graphs && it > 0) {
+        } else if (graphs && it >= warm_iters) {
             save_state();
             cudaGraph_t g = nullptr;
             cudaError_t ec = cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeRelaxed);
@@ -1363,7 +1371,7 @@ struct CpSession {
 
     // The remaining iterations can run as a device-side loop.
     bool loop_eligible() const {
-        return graphs && !done && it == 1 && !o.verbose &&
+        return graphs && !done && it == warm_iters && !o.verbose && self_map &&
                (p.layout == DGPU_LAYOUT_NCOPY || p.cur == cur_start);
     }
 
@@ -1632,7 +1640,15 @@ int cpals_run(Plan& p, const dgpu_cp_options& o, dgpu_cp_result& res, double* fi
             replayed = true;
         }
     }
-    if (!replayed && !s.done) DGPU_TRY(s.step_host());
+    if (!replayed && !s.done) {
+        const uint64_t unc0 = p.pc_uncached;
+        DGPU_TRY(s.step_host());
+        s.self_map = p.layout == DGPU_LAYOUT_NCOPY || p.cur == s.cur_start;
+        if (s.graphs && p.pc_uncached != unc0 && !s.done) {
+            s.warm_iters = 2;
+            DGPU_TRY(s.step_host());
+        }
+    }
     if (!replayed && s.loop_eligible()) DGPU_TRY(run_loop_cached(s));
     while (!s.done) DGPU_TRY(s.step_host());
     s.finish();

@@ -99,6 +99,26 @@ struct PartList {
     bool      own_tiles = false;
 };
 
+// Offset tables of one partition pass of the PingPong sweep, kept for the
+// next sweep.  After the slab has gone through one full cycle of modes its
+// arrangement is a function of the coordinates alone (every mode's shard and
+// row key plus the schedule order break all ties), so each pass of a later
+// cycle sees the same arrangement and produces the same per-(chunk, bucket)
+// offsets; the reference likewise builds its remap cursor table once, at
+// preprocessing.  Valid while the pass runs with the same list, key and
+// bucket count.
+constexpr int kPartCachePasses = 4;            // LSD passes per sort kept
+struct PartCacheSlot {
+    uint32_t*       off = nullptr;             // [chunks x buckets] in-segment prefixes
+    uint32_t*       base = nullptr;            // [segments x buckets] bucket starts
+    size_t          off_cap = 0, base_cap = 0; // entries allocated
+    const PartList* list = nullptr;
+    uint64_t        lists_gen = 0;
+    int             key_mode = -1, shift = -1;
+    uint32_t        mask = 0, nb = 0;
+    bool            valid = false;
+};
+
 // SoA slab on the device.
 struct Slab {
     void*     raw = nullptr;
@@ -233,6 +253,19 @@ struct Plan {
     size_t       part_cap = 0;                  // entries of each
     uint32_t*    part_base = nullptr;           // [segments x buckets] bucket starts
     size_t       part_base_cap = 0;
+    // PingPong partition passes: offset tables kept per (mode, fiber sort 0 /
+    // remap 1, LSD pass) once the slab is past its first cycle (see
+    // PartCacheSlot); DGPU_PART_CACHE=0 turns this off and
+    // DGPU_PART_CACHE_CHECK=1 recomputes every kept table and flags a
+    // difference (device fault flag 0x1000)
+    PartCacheSlot pcache[kMaxModes][2][kPartCachePasses];
+    int          part_cache = 1;
+    int          part_cache_check = 0;
+    uint64_t     pp_transitions = 0;            // PingPong modes run since the slab was set
+    uint64_t     lists_gen = 0;                 // bumped when partition lists are rebuilt
+    uint64_t     pc_uncached = 0;               // PingPong passes that computed their tables
+    int          pc_mode = -1;                  // mode of the running PingPong step (-1: none)
+    PartCacheSlot* pc_slot = nullptr;           // slot of the next stable_partition call
     int*         err_flag = nullptr;            // device-side fault flag
     uint32_t*    part_ctr = nullptr;            // work-queue counter of the partition scatter
     float*       lambda = nullptr;              // [Rp]

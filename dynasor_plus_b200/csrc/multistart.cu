@@ -596,6 +596,7 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
         (p.layout == DGPU_LAYOUT_NCOPY || p.cur == cur_start)) {
         // remaining iterations: one graph launch with a device-side loop
         const int cur0 = p.cur, nm0 = p.next_mode;
+        const uint64_t pp0 = p.pp_transitions;
         bool stale0[kMaxModes];
         for (int n = 0; n < kMaxModes; ++n) stale0[n] = p.yb_stale[n];
         cudaGraph_t outer = nullptr;
@@ -638,6 +639,7 @@ int cpals_multistart_run(Plan& p, int K, const dgpu_cp_options& o, dgpu_cp_resul
             cudaGetLastError();
             p.cur = cur0;
             p.next_mode = nm0;
+            p.pp_transitions = pp0;
             for (int n = 0; n < kMaxModes; ++n) p.yb_stale[n] = stale0[n];
         }
     }

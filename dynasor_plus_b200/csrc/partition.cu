@@ -264,6 +264,19 @@ __device__ __forceinline__ void fence_mbar_init() {
 // Device fault-flag codes written by the partition kernels.
 constexpr int kErrPartWait = 0x100;      // a bulk copy did not complete in time
 constexpr int kErrPartRange = 0x200;     // a slot outside its window or slab (skipped)
+constexpr int kErrPartCache = 0x1000;    // a kept offset table differs from a recomputed one
+
+// Flags kErrPartCache where a[i] != b[i] (check mode of the kept tables).
+__global__ void k_cmp_tables(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                             size_t n, int* __restrict__ err)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        if (a[i] != b[i]) {
+            atomicOr(err, kErrPartCache);
+            return;
+        }
+}
 
 // Tile descriptors of a chunk that a scatter CTA copies to shared memory
 // when it takes the chunk (a chunk with more tiles reads the rest from
@@ -656,7 +669,8 @@ int ensure_part_scratch(Plan& p, size_t entries, size_t base_entries) {
 
 template <int N>
 int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, int key_mode,
-                   int key_shift, uint32_t key_mask, uint32_t nb)
+                   int key_shift, uint32_t key_mask, uint32_t nb, const uint32_t* off,
+                   const uint32_t* base)
 {
     constexpr int W = scatter_window<N>();
     const size_t smem = scatter_smem<N>(nb);
@@ -685,8 +699,8 @@ int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, 
     const uint32_t grid = std::max(1u, std::min(L.nchunks, (uint32_t)(std::max(1, per_sm) * p.sms)));
     DGPU_CUDA(cudaMemsetAsync(p.part_ctr, 0, sizeof(uint32_t), p.stream));
     k_chunk_scatter<N, W><<<grid, kScatThreads, smem, p.stream>>>(
-        slab_in(in, p.N), slab_out(out, p.N), L.tiles, L.chunks, L.order, L.nchunks, p.part_off,
-        p.part_base, key_mode, key_shift, key_mask, nb, (uint32_t)p.nnz, p.part_ctr, p.err_flag);
+        slab_in(in, p.N), slab_out(out, p.N), L.tiles, L.chunks, L.order, L.nchunks, off,
+        base, key_mode, key_shift, key_mask, nb, (uint32_t)p.nnz, p.part_ctr, p.err_flag);
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
 }
@@ -791,17 +805,45 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     return DGPU_OK;
 }
 
-int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, int key_shift,
-                     uint32_t key_mask, uint32_t nb, const Slab& out)
+// Histogram + scans of one partition pass.  The offsets go to the plan's
+// shared scratch, or, given a cache slot that is not valid while the stream
+// is not being captured, to the slot, which becomes valid.  In check mode a
+// valid slot's tables are compared with freshly computed ones (fault flag
+// kErrPartCache on a difference).  *off / *base receive the tables to use.
+static int compute_offsets(Plan& p, const Slab& in, const PartList& L, int key_mode,
+                           int key_shift, uint32_t key_mask, uint32_t nb, PartCacheSlot* cs,
+                           bool hit, const uint32_t** off_out, const uint32_t** base_out)
 {
-    if (L.nchunks == 0) return DGPU_OK;
-    if (nb == 0 || nb > kMaxBuckets) {
-        set_error("stable_partition: %u buckets (max %u)", nb, kMaxBuckets);
-        return DGPU_ERR_ARG;
+    const size_t off_n = (size_t)L.nchunks * nb, base_n = (size_t)L.nsegs * nb;
+    DGPU_TRY(ensure_part_scratch(p, off_n, base_n));
+    uint32_t* off = p.part_off;
+    uint32_t* base = p.part_base;
+    bool fill = false;
+    if (cs && !hit) {
+        cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+        DGPU_CUDA(cudaStreamIsCapturing(p.stream, &cst));
+        if (cst == cudaStreamCaptureStatusNone) {
+            cs->valid = false;
+            if (cs->off_cap < off_n) {
+                dev_free(cs->off);
+                cs->off = nullptr;
+                cs->off_cap = 0;
+                DGPU_TRY(dev_alloc(p, (void**)&cs->off, off_n * sizeof(uint32_t)));
+                cs->off_cap = off_n;
+            }
+            if (cs->base_cap < base_n) {
+                dev_free(cs->base);
+                cs->base = nullptr;
+                cs->base_cap = 0;
+                DGPU_TRY(dev_alloc(p, (void**)&cs->base, base_n * sizeof(uint32_t)));
+                cs->base_cap = base_n;
+            }
+            off = cs->off;
+            base = cs->base;
+            fill = true;
+        }
     }
-    DGPU_TRY(ensure_part_scratch(p, (size_t)L.nchunks * nb, (size_t)L.nsegs * nb));
     const double elem = (double)p.nnz;
-    const double row_bytes = 4.0 + 4.0 * p.N;
     {
         LaunchTimer t(p, p.part_fiber ? KK_FIB_HIST : KK_PART_HIST,
                       elem * 4.0 + (double)L.nchunks * nb * 4.0);
@@ -815,20 +857,75 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
     {
         LaunchTimer t(p, p.part_fiber ? KK_FIB_SCAN : KK_PART_SCAN, (double)L.nchunks * nb * 8.0);
         dim3 g(L.nsegs, (nb + 31) / 32);
-        k_col_scan<<<g, 1024, 0, p.stream>>>(p.part_cnt, L.segs, nb, p.part_off, p.part_base);
-        k_bucket_scan<<<L.nsegs, 1024, 0, p.stream>>>(p.part_base, L.segs, nb);
+        k_col_scan<<<g, 1024, 0, p.stream>>>(p.part_cnt, L.segs, nb, off, base);
+        k_bucket_scan<<<L.nsegs, 1024, 0, p.stream>>>(base, L.segs, nb);
         DGPU_CUDA(cudaGetLastError());
     }
+    if (hit) {
+        // check mode: the kept tables must equal this sweep's
+        const uint32_t grid = (uint32_t)std::min<size_t>(4u * (uint32_t)p.sms, (off_n + 255) / 256);
+        k_cmp_tables<<<std::max(1u, grid), 256, 0, p.stream>>>(cs->off, off, off_n, p.err_flag);
+        k_cmp_tables<<<1, 256, 0, p.stream>>>(cs->base, base, base_n, p.err_flag);
+        DGPU_CUDA(cudaGetLastError());
+    }
+    if (fill) {
+        cs->valid = true;
+        cs->list = &L;
+        cs->lists_gen = p.lists_gen;
+        cs->key_mode = key_mode;
+        cs->shift = key_shift;
+        cs->mask = key_mask;
+        cs->nb = nb;
+        ++p.tables_gen;              // graphs kept over older tables recapture
+    }
+    *off_out = off;
+    *base_out = base;
+    return DGPU_OK;
+}
+
+int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, int key_shift,
+                     uint32_t key_mask, uint32_t nb, const Slab& out)
+{
+    PartCacheSlot* cs = p.pc_slot;
+    p.pc_slot = nullptr;
+    if (L.nchunks == 0) return DGPU_OK;
+    if (nb == 0 || nb > kMaxBuckets) {
+        set_error("stable_partition: %u buckets (max %u)", nb, kMaxBuckets);
+        return DGPU_ERR_ARG;
+    }
+    // a PingPong pass past the slab's first cycle reuses its kept tables
+    const bool hit = cs && cs->valid && cs->list == &L && cs->lists_gen == p.lists_gen &&
+                     cs->key_mode == key_mode && cs->shift == key_shift &&
+                     cs->mask == key_mask && cs->nb == nb;
+    const uint32_t* off = nullptr;
+    const uint32_t* base = nullptr;
+    if (hit && !p.part_cache_check) {
+        off = cs->off;
+        base = cs->base;
+    } else {
+        DGPU_TRY(compute_offsets(p, in, L, key_mode, key_shift, key_mask, nb, cs, hit, &off, &base));
+        // a PingPong pass whose tables are not kept for the next sweep
+        if (p.pc_mode >= 0 && !(cs && cs->valid)) ++p.pc_uncached;
+    }
+    const double row_bytes = 4.0 + 4.0 * p.N;
     LaunchTimer t(p, p.part_fiber ? KK_FIB_SCATTER : KK_PART_SCATTER,
-                  elem * 2.0 * row_bytes + (double)L.nchunks * nb * 4.0);
+                  (double)p.nnz * 2.0 * row_bytes + (double)L.nchunks * nb * 4.0);
     switch (p.N) {
-#define DGPU_SC(NN) case NN: return launch_scatter<NN>(p, in, out, L, key_mode, key_shift, key_mask, nb)
+#define DGPU_SC(NN) case NN: return launch_scatter<NN>(p, in, out, L, key_mode, key_shift, key_mask, nb, off, base)
         DGPU_SC(2); DGPU_SC(3); DGPU_SC(4); DGPU_SC(5); DGPU_SC(6); DGPU_SC(7); DGPU_SC(8);
 #undef DGPU_SC
         default:
             set_error("stable_partition: %d modes unsupported", p.N);
             return DGPU_ERR_ARG;
     }
+}
+
+// The kept-table slot of LSD pass k of the running PingPong step's fiber
+// sort (kind 0) or remap (kind 1); none outside a PingPong step, before the
+// slab has been through one cycle of modes, or with the cache off.
+static PartCacheSlot* cache_slot(Plan& p, int kind, int k) {
+    if (p.pc_mode < 0 || k >= kPartCachePasses || p.pp_transitions < (uint64_t)p.N) return nullptr;
+    return &p.pcache[p.pc_mode][kind][k];
 }
 
 int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first, int key_mode,
@@ -854,6 +951,7 @@ int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first, int key_m
             nb = (uint32_t)std::min<uint64_t>((uint64_t)mask + 1, top + 1);
         }
         const PartList& L = (k == 0) ? first : p.ident;
+        p.pc_slot = cache_slot(p, 1, k);
         DGPU_TRY(stable_partition(p, p.slab[src], L, key_mode, sh, mask, nb, p.slab[dst]));
         std::swap(src, dst);
     }
@@ -880,6 +978,7 @@ int fiber_sort(Plan& p, int n, int src, int other, int* result) {
         const int sh = k * dbits;
         const int hi = std::min(bits, sh + dbits);
         const uint32_t mask = (1u << (hi - sh)) - 1u;
+        p.pc_slot = cache_slot(p, 0, k);
         const int rc = stable_partition(p, p.slab[a], p.fib[n], n, sh, mask, mask + 1, p.slab[b]);
         if (rc != DGPU_OK) { p.part_fiber = 0; return rc; }
         std::swap(a, b);

@@ -94,7 +94,8 @@ int sync_checked(Plan& p) {
         set_error("device fault flag 0x%x: %s", flag,
                   (flag & 0x100) ? "a partition kernel's bulk copy did not complete in time"
                   : (flag & 0x200) ? "a partition kernel computed an out-of-range slot"
-                                   : "a device-side check failed");
+                  : (flag & 0x1000) ? "a kept partition offset table differs from a recomputed one"
+                                    : "a device-side check failed");
         return DGPU_ERR_DEVICE;
     }
     return DGPU_OK;
@@ -189,6 +190,12 @@ Plan::~Plan() {
     dev_free(part_cnt);
     dev_free(part_off);
     dev_free(part_base);
+    for (auto& per_mode : pcache)
+        for (auto& per_kind : per_mode)
+            for (PartCacheSlot& c : per_kind) {
+                dev_free(c.off);
+                dev_free(c.base);
+            }
     dev_free(err_flag);
     dev_free(part_ctr);
     dev_free(lambda);
@@ -400,6 +407,8 @@ static int plan_init(Plan& p, int N, uint64_t nnz, const uint32_t* dims, const d
     if (const char* e = std::getenv("DGPU_MTTKRP_KERNEL")) p.mttkrp_kernel = std::atoi(e) == 1 ? 1 : 0;
     if (const char* e = std::getenv("DGPU_RANK_TILE")) p.rank_tile = std::atoi(e);
     if (const char* e = std::getenv("DGPU_OVERLAP")) p.overlap = std::atoi(e);
+    if (const char* e = std::getenv("DGPU_PART_CACHE")) p.part_cache = std::atoi(e) != 0 ? 1 : 0;
+    if (const char* e = std::getenv("DGPU_PART_CACHE_CHECK")) p.part_cache_check = std::atoi(e) != 0 ? 1 : 0;
     for (int n = 0; n < N; ++n) p.dims[n] = dims[n];
     return DGPU_OK;
 }
@@ -500,6 +509,7 @@ int plan_rebuild_partlists(Plan& p) {
     // plan's, and bump the generation that every cached key carries (a
     // batch graph kept on another plan then no longer matches)
     ++p.tables_gen;
+    ++p.lists_gen;                               // kept partition tables no longer match
     if (p.cp_loop_exec) { cudaGraphExecDestroy(p.cp_loop_exec); p.cp_loop_exec = nullptr; }
     if (p.cp_batch_exec) { cudaGraphExecDestroy(p.cp_batch_exec); p.cp_batch_exec = nullptr; }
     DGPU_CUDA(cudaStreamSynchronize(p.stream));
@@ -590,6 +600,7 @@ int plan_build(Plan& p, const dgpu_tensor_desc& t, const dgpu_plan_opts& o) {
     DGPU_TRY(stable_sort_pingpong(p, in_slab, 0, p.ident, 0, p.shift[0], p.K[0], &res));
     p.cur = res;
     p.next_mode = 0;
+    p.pp_transitions = 0;
 
     if (p.layout == DGPU_LAYOUT_NCOPY) {
         // copy 0 lives in slab[0]; copy k = remap of copy k-1 by the mode
@@ -721,6 +732,7 @@ static int plan_build_dnp_morton(Plan& p, const DnpImage& img, const dgpu_plan_o
     free_slabs(p);
     p.cur = 0;
     p.next_mode = 0;
+    p.pp_transitions = 0;
     DGPU_TRY(plan_factors(p));
     DGPU_TRY(sync_checked(p));
     return DGPU_OK;
@@ -861,6 +873,12 @@ static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwai
                   "order 0..N-1", n, p.next_mode);
         return DGPU_ERR_ORDER;
     }
+    // the step's partition passes may use kept offset tables (stable_partition)
+    struct PcScope {
+        Plan& p;
+        PcScope(Plan& q, int n) : p(q) { p.pc_mode = q.part_cache ? n : -1; }
+        ~PcScope() { p.pc_mode = -1; p.pc_slot = nullptr; }
+    } pc_scope(p, n);
     const int other = 1 - p.cur;
     if (p.fiber && p.kclass[n] == 2) {
         int r = 0;
@@ -924,6 +942,7 @@ static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwai
     }
     p.cur = r;
     p.next_mode = nm;
+    ++p.pp_transitions;
     return DGPU_OK;
 }
 
