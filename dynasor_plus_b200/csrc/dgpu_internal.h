@@ -97,6 +97,13 @@ struct PartList {
     uint32_t  nsegs = 0;
     uint32_t* order = nullptr;    // chunk ids, largest first: the scatter's work queue
     bool      own_tiles = false;
+    // the scatter's windows in list order (a window never crosses a tile):
+    // {first slab position, offset in list order, element count, 0}, and
+    // each tile's offset in list order
+    uint4*    wins = nullptr;
+    uint32_t  nwin = 0;
+    uint32_t* tile_pre = nullptr;
+    uint64_t  total = 0;          // elements listed
 };
 
 // Offset tables of one partition pass of the PingPong sweep, kept for the
@@ -117,6 +124,13 @@ struct PartCacheSlot {
     int             key_mode = -1, shift = -1;
     uint32_t        mask = 0, nb = 0;
     bool            valid = false;
+    // the pass recorded element by element (list order): each element's
+    // slot in its window's bucket-ordered staging, and each staged slot's
+    // destination; a pass with a recording is replayed without ranking
+    uint16_t*       lp = nullptr;
+    uint32_t*       dst = nullptr;
+    size_t          rec_cap = 0;               // elements of lp / dst
+    bool            replay = false;
 };
 
 // SoA slab on the device.
@@ -261,6 +275,7 @@ struct Plan {
     PartCacheSlot pcache[kMaxModes][2][kPartCachePasses];
     int          part_cache = 1;
     int          part_cache_check = 0;
+    int          part_replay = 1;               // DGPU_PART_REPLAY=0: kept tables only, no recording
     uint64_t     pp_transitions = 0;            // PingPong modes run since the slab was set
     uint64_t     lists_gen = 0;                 // bumped when partition lists are rebuilt
     uint64_t     pc_uncached = 0;               // PingPong passes that computed their tables

@@ -39,6 +39,7 @@
 #include "dgpu_internal.h"
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <numeric>
 
@@ -371,14 +372,16 @@ constexpr int scatter_bufs() { return scatter_cols<N>() <= 4 ? 3 : 2; }
 //      destination, in the buffer it came from; warps reset their counters;
 //   d. the staged window is written out: consecutive threads store
 //      consecutive slots of one bucket.
-template <int N, int W>
+template <int N, int W, bool REC>
 __global__ void __launch_bounds__(kScatThreads, DGPU_SCAT_MINB)
 k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
                 const Tile* __restrict__ tiles, const Chunk* __restrict__ chunks,
                 const uint32_t* __restrict__ order, uint32_t nchunks,
                 const uint32_t* __restrict__ off, const uint32_t* __restrict__ base,
                 int key_mode, int shift, uint32_t mask, uint32_t nb, uint32_t total,
-                uint32_t* __restrict__ queue, int* __restrict__ err)
+                uint32_t* __restrict__ queue, int* __restrict__ err,
+                const uint32_t* __restrict__ tile_pre, uint16_t* __restrict__ rec_lp,
+                uint32_t* __restrict__ rec_dst)
 {
     constexpr int S = W / kScatThreads;           // steps per warp per window
     constexpr int PW = W / kScatWarps;            // elements per warp per window
@@ -575,12 +578,16 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                 }
             }
             __syncthreads();       // (3)
-            // c. stage in bucket order
+            // c. stage in bucket order (REC: each element's slot is recorded
+            //    at its list-order position)
+            uint32_t ro = 0;
+            if constexpr (REC) ro = tile_pre[t] + w0;
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
                 const uint32_t lp = wbase[key[s]] + wc[wc_slot(key[s], warp)] + rk[s];
                 if (lp >= cnt) { atomicOr(err, kErrPartRange); continue; }
+                if constexpr (REC) rec_lp[ro + warp * PW + s * 32 + lane] = (uint16_t)lp;
                 if constexpr (kRec) {
                     uint32_t r[4] = {__float_as_uint(val[s]), 0u, 0u, 0u};
 #pragma unroll
@@ -608,6 +615,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                     const uint32_t kb = part_key(kv, shift, mask);
                     const uint32_t d = kb < nb ? wdst[kb] + i : total;
                     if (d >= total) { atomicOr(err, kErrPartRange); continue; }
+                    if constexpr (REC) rec_dst[ro + i] = d;
                     out.vals[d] = __uint_as_float(rv[0]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = rv[m + 1];
@@ -615,6 +623,7 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                     const uint32_t kb = part_key(bk[(size_t)(key_mode + 1) * BW + i], shift, mask);
                     const uint32_t d = kb < nb ? wdst[kb] + i : total;
                     if (d >= total) { atomicOr(err, kErrPartRange); continue; }
+                    if constexpr (REC) rec_dst[ro + i] = d;
                     out.vals[d] = __uint_as_float(bk[i]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = bk[(size_t)(m + 1) * BW + i];
@@ -639,6 +648,82 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 }
 
 
+
+// Replay of a recorded pass: the window list in order, grid-strided (the
+// destinations are recorded, so windows are independent).  Per window each
+// thread loads its elements and stores them at their recorded staging slots
+// (a 16-byte record when N <= 3, else one word per column), then writes
+// staged slot i to its recorded destination: the same bucket-ordered runs
+// the ranked scatter writes, without its ranking, counters and prefixes.
+constexpr int kReplayThreads = 256;
+template <int N, int W>
+__global__ void __launch_bounds__(kReplayThreads)
+k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
+              const uint4* __restrict__ wins, uint32_t nwin, const uint16_t* __restrict__ lp,
+              const uint32_t* __restrict__ dst, uint32_t total, int* __restrict__ err)
+{
+    constexpr int U = W / kReplayThreads;         // elements per thread per window
+    constexpr bool kRec = (N + 1 <= 4);
+    extern __shared__ __align__(16) uint32_t sm[];   // [W] records or [N+1][W] columns
+    for (uint32_t w = blockIdx.x; w < nwin; w += gridDim.x) {
+        const uint4 d = wins[w];                  // {src, list offset, count, -}
+        const uint32_t cnt = min(d.z, (uint32_t)W);
+        uint32_t slot[U];
+        float val[U];
+        uint32_t id[U][N];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = u * kReplayThreads + threadIdx.x;
+            slot[u] = 0xffffffffu;
+            if (j < cnt) {
+                slot[u] = lp[d.y + j];
+                val[u] = in.vals[d.x + j];
+#pragma unroll
+                for (int m = 0; m < N; ++m) id[u][m] = in.idx[m][d.x + j];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (slot[u] == 0xffffffffu) continue;
+            if (slot[u] >= cnt) { atomicOr(err, kErrPartRange); continue; }
+            if constexpr (kRec) {
+                uint32_t r[4] = {__float_as_uint(val[u]), 0u, 0u, 0u};
+#pragma unroll
+                for (int m = 0; m < N; ++m) r[m + 1] = id[u][m];
+                reinterpret_cast<uint4*>(sm)[slot[u]] = make_uint4(r[0], r[1], r[2], r[3]);
+            } else {
+                sm[slot[u]] = __float_as_uint(val[u]);
+#pragma unroll
+                for (int m = 0; m < N; ++m) sm[(size_t)(m + 1) * W + slot[u]] = id[u][m];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t i = u * kReplayThreads + threadIdx.x;
+            if (i >= cnt) break;
+            const uint32_t g = dst[d.y + i];
+            if (g >= total) { atomicOr(err, kErrPartRange); continue; }
+            if constexpr (kRec) {
+                const uint4 r = reinterpret_cast<const uint4*>(sm)[i];
+                const uint32_t rv[4] = {r.x, r.y, r.z, r.w};
+                out.vals[g] = __uint_as_float(rv[0]);
+#pragma unroll
+                for (int m = 0; m < N; ++m) out.idx[m][g] = rv[m + 1];
+            } else {
+                out.vals[g] = __uint_as_float(sm[i]);
+#pragma unroll
+                for (int m = 0; m < N; ++m) out.idx[m][g] = sm[(size_t)(m + 1) * W + i];
+            }
+        }
+        __syncthreads();                          // staging reused by the next window
+    }
+}
+
+template <int N>
+constexpr size_t replay_smem() {
+    return (N + 1 <= 4 ? 4 : N + 1) * (size_t)scatter_window<N>() * sizeof(uint32_t);
+}
 
 template <int N>
 size_t scatter_smem(uint32_t nb) {
@@ -667,42 +752,70 @@ int ensure_part_scratch(Plan& p, size_t entries, size_t base_entries) {
     return DGPU_OK;
 }
 
+// Raises kernel `k`'s dynamic shared memory limit on this device (function
+// attributes are per context) to `smem` if it is below (the limit only
+// grows; guarded because plans may be driven from several host threads).
+// Kept per (kernel, device): instantiations share a function type.
+template <typename K>
+int ensure_smem_limit(K* k, size_t smem, int device) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> have;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& h = have[std::make_pair(reinterpret_cast<const void*>(k), device)];
+    if (smem <= h) return DGPU_OK;
+    if (smem > 227u * 1024u) {
+        set_error("stable_partition: a pass needs %zu bytes of shared memory", smem);
+        return DGPU_ERR_ARG;
+    }
+    DGPU_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    h = smem;
+    return DGPU_OK;
+}
+
+// The ranked scatter of one pass; with `rec` it also records the pass into
+// rec's slot and destination arrays.
 template <int N>
 int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, int key_mode,
                    int key_shift, uint32_t key_mask, uint32_t nb, const uint32_t* off,
-                   const uint32_t* base)
+                   const uint32_t* base, const PartCacheSlot* rec)
 {
     constexpr int W = scatter_window<N>();
     const size_t smem = scatter_smem<N>(nb);
-    // dynamic shared memory limit, raised per device (function attributes are
-    // per context) to the largest request seen so far
-    // (the limit only grows; guarded because plans may be driven from
-    // several host threads)
-    static std::mutex mu;
-    static size_t attr_bytes[64] = {};
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        size_t& have = attr_bytes[p.device & 63];
-        if (smem > have) {
-            if (smem > 227u * 1024u) {
-                set_error("stable_partition: %u buckets need %zu bytes of shared memory", nb, smem);
-                return DGPU_ERR_ARG;
-            }
-            DGPU_CUDA(cudaFuncSetAttribute(k_chunk_scatter<N, W>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            have = smem;
-        }
-    }
+    auto* kern = rec ? k_chunk_scatter<N, W, true> : k_chunk_scatter<N, W, false>;
+    DGPU_TRY(ensure_smem_limit(kern, smem, p.device));
     int per_sm = 0;
-    DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chunk_scatter<N, W>,
-                                                            kScatThreads, smem));
+    DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScatThreads, smem));
     const uint32_t grid = std::max(1u, std::min(L.nchunks, (uint32_t)(std::max(1, per_sm) * p.sms)));
     DGPU_CUDA(cudaMemsetAsync(p.part_ctr, 0, sizeof(uint32_t), p.stream));
-    k_chunk_scatter<N, W><<<grid, kScatThreads, smem, p.stream>>>(
+    kern<<<grid, kScatThreads, smem, p.stream>>>(
         slab_in(in, p.N), slab_out(out, p.N), L.tiles, L.chunks, L.order, L.nchunks, off,
-        base, key_mode, key_shift, key_mask, nb, (uint32_t)p.nnz, p.part_ctr, p.err_flag);
+        base, key_mode, key_shift, key_mask, nb, (uint32_t)p.nnz, p.part_ctr, p.err_flag,
+        L.tile_pre, rec ? rec->lp : nullptr, rec ? rec->dst : nullptr);
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
+}
+
+template <int N>
+int launch_replay(Plan& p, const Slab& in, const Slab& out, const PartList& L,
+                  const PartCacheSlot& cs)
+{
+    constexpr int W = scatter_window<N>();
+    constexpr size_t smem = replay_smem<N>();
+    auto* kern = k_part_replay<N, W>;
+    DGPU_TRY(ensure_smem_limit(kern, smem, p.device));
+    int per_sm = 0;
+    DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kReplayThreads, smem));
+    const uint32_t grid = std::max(1u, std::min(L.nwin, (uint32_t)(std::max(1, per_sm) * p.sms)));
+    kern<<<grid, kReplayThreads, smem, p.stream>>>(slab_in(in, p.N), slab_out(out, p.N), L.wins,
+                                                   L.nwin, cs.lp, cs.dst, (uint32_t)p.nnz,
+                                                   p.err_flag);
+    DGPU_CUDA(cudaGetLastError());
+    return DGPU_OK;
+}
+
+// Window size of the scatter for N modes (host side).
+uint32_t scatter_window_host(int N) {
+    return N <= 4 ? (uint32_t)DGPU_SCAT_WINDOW : (uint32_t)DGPU_SCAT_WINDOW / 2u;
 }
 
 }  // namespace
@@ -712,6 +825,8 @@ void free_partlist(PartList& l) {
     dev_free(l.chunks);
     dev_free(l.segs);
     dev_free(l.order);
+    dev_free(l.wins);
+    dev_free(l.tile_pre);
     l = PartList{};
 }
 
@@ -777,6 +892,21 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t a, uint32_t b) { return csize[a] > csize[b]; });
+    // the scatter's windows (W-element pieces of each tile) and tile offsets
+    // in list order: the layout of a recorded pass
+    const uint32_t W = scatter_window_host(p.N);
+    std::vector<uint32_t> pre(tiles.size());
+    std::vector<uint4> wins;
+    uint64_t acc = 0;
+    for (size_t t = 0; t < tiles.size(); ++t) {
+        pre[t] = (uint32_t)acc;
+        for (uint32_t w0 = 0; w0 < tiles[t].count; w0 += W)
+            wins.push_back(make_uint4(tiles[t].begin + w0, (uint32_t)acc + w0,
+                                      std::min(W, tiles[t].count - w0), 0u));
+        acc += tiles[t].count;
+    }
+    out.total = acc;
+    out.nwin = (uint32_t)wins.size();
     out.ntiles = (uint32_t)tiles.size();
     out.nchunks = (uint32_t)ch.size();
     out.nsegs = (uint32_t)sg.size();
@@ -793,6 +923,14 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     DGPU_TRY(dev_alloc(p, (void**)&out.chunks, std::max<size_t>(1, ch.size()) * sizeof(Chunk)));
     DGPU_TRY(dev_alloc(p, (void**)&out.segs, std::max<size_t>(1, sg.size()) * sizeof(Seg)));
     DGPU_TRY(dev_alloc(p, (void**)&out.order, std::max<size_t>(1, ch.size()) * sizeof(uint32_t)));
+    DGPU_TRY(dev_alloc(p, (void**)&out.wins, std::max<size_t>(1, wins.size()) * sizeof(uint4)));
+    DGPU_TRY(dev_alloc(p, (void**)&out.tile_pre, std::max<size_t>(1, pre.size()) * sizeof(uint32_t)));
+    if (!wins.empty())
+        DGPU_CUDA(cudaMemcpyAsync(out.wins, wins.data(), wins.size() * sizeof(uint4),
+                                  cudaMemcpyHostToDevice, p.stream));
+    if (!pre.empty())
+        DGPU_CUDA(cudaMemcpyAsync(out.tile_pre, pre.data(), pre.size() * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice, p.stream));
     if (!ch.empty()) {
         DGPU_CUDA(cudaMemcpyAsync(out.chunks, ch.data(), ch.size() * sizeof(Chunk),
                                   cudaMemcpyHostToDevice, p.stream));
@@ -805,6 +943,33 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     return DGPU_OK;
 }
 
+// Recording buffers of a slot (one 2-byte slot and one 4-byte destination
+// per listed element), grown only while the device keeps at least a quarter
+// of its memory free; a slot without them runs its ranked scatter on the
+// kept tables.
+static int reserve_recording(Plan& p, const PartList& L, PartCacheSlot& cs) {
+    if (cs.rec_cap >= L.total) return DGPU_OK;
+    dev_free(cs.lp);
+    dev_free(cs.dst);
+    cs.lp = nullptr;
+    cs.dst = nullptr;
+    cs.rec_cap = 0;
+    size_t free_b = 0, total_b = 0;
+    DGPU_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t need = (size_t)L.total * (sizeof(uint16_t) + sizeof(uint32_t)) + 512;
+    if (free_b < need || free_b - need < total_b / 4) return DGPU_OK;
+    if (dev_alloc(p, (void**)&cs.lp, (size_t)L.total * sizeof(uint16_t)) != DGPU_OK ||
+        dev_alloc(p, (void**)&cs.dst, (size_t)L.total * sizeof(uint32_t)) != DGPU_OK) {
+        dev_free(cs.lp);
+        dev_free(cs.dst);
+        cs.lp = nullptr;
+        cs.dst = nullptr;
+        return DGPU_OK;                          // no recording: not an error
+    }
+    cs.rec_cap = L.total;
+    return DGPU_OK;
+}
+
 // Histogram + scans of one partition pass.  The offsets go to the plan's
 // shared scratch, or, given a cache slot that is not valid while the stream
 // is not being captured, to the slot, which becomes valid.  In check mode a
@@ -812,8 +977,10 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
 // kErrPartCache on a difference).  *off / *base receive the tables to use.
 static int compute_offsets(Plan& p, const Slab& in, const PartList& L, int key_mode,
                            int key_shift, uint32_t key_mask, uint32_t nb, PartCacheSlot* cs,
-                           bool hit, const uint32_t** off_out, const uint32_t** base_out)
+                           bool hit, const uint32_t** off_out, const uint32_t** base_out,
+                           bool* filled)
 {
+    *filled = false;
     const size_t off_n = (size_t)L.nchunks * nb, base_n = (size_t)L.nsegs * nb;
     DGPU_TRY(ensure_part_scratch(p, off_n, base_n));
     uint32_t* off = p.part_off;
@@ -876,7 +1043,9 @@ static int compute_offsets(Plan& p, const Slab& in, const PartList& L, int key_m
         cs->shift = key_shift;
         cs->mask = key_mask;
         cs->nb = nb;
+        cs->replay = false;
         ++p.tables_gen;              // graphs kept over older tables recapture
+        *filled = true;
     }
     *off_out = off;
     *base_out = base;
@@ -899,25 +1068,48 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
                      cs->mask == key_mask && cs->nb == nb;
     const uint32_t* off = nullptr;
     const uint32_t* base = nullptr;
+    const PartCacheSlot* rec = nullptr;       // record this pass into the slot
     if (hit && !p.part_cache_check) {
         off = cs->off;
         base = cs->base;
     } else {
-        DGPU_TRY(compute_offsets(p, in, L, key_mode, key_shift, key_mask, nb, cs, hit, &off, &base));
+        bool filled = false;
+        DGPU_TRY(compute_offsets(p, in, L, key_mode, key_shift, key_mask, nb, cs, hit, &off, &base,
+                                 &filled));
         // a PingPong pass whose tables are not kept for the next sweep
         if (p.pc_mode >= 0 && !(cs && cs->valid)) ++p.pc_uncached;
+        if (filled && p.part_replay) {
+            DGPU_TRY(reserve_recording(p, L, *cs));
+            if (cs->rec_cap >= L.total) rec = cs;
+        }
     }
     const double row_bytes = 4.0 + 4.0 * p.N;
+    const double elem = (double)L.total;
+    if (hit && cs->replay) {
+        LaunchTimer t(p, p.part_fiber ? KK_FIB_SCATTER : KK_PART_SCATTER,
+                      elem * (2.0 * row_bytes + 6.0));
+        switch (p.N) {
+#define DGPU_RP(NN) case NN: return launch_replay<NN>(p, in, out, L, *cs)
+            DGPU_RP(2); DGPU_RP(3); DGPU_RP(4); DGPU_RP(5); DGPU_RP(6); DGPU_RP(7); DGPU_RP(8);
+#undef DGPU_RP
+            default: break;
+        }
+        set_error("stable_partition: %d modes unsupported", p.N);
+        return DGPU_ERR_ARG;
+    }
     LaunchTimer t(p, p.part_fiber ? KK_FIB_SCATTER : KK_PART_SCATTER,
-                  (double)p.nnz * 2.0 * row_bytes + (double)L.nchunks * nb * 4.0);
+                  elem * 2.0 * row_bytes + (double)L.nchunks * nb * 4.0);
+    int rc = DGPU_ERR_ARG;
     switch (p.N) {
-#define DGPU_SC(NN) case NN: return launch_scatter<NN>(p, in, out, L, key_mode, key_shift, key_mask, nb, off, base)
+#define DGPU_SC(NN) case NN: rc = launch_scatter<NN>(p, in, out, L, key_mode, key_shift, key_mask, nb, off, base, rec); break
         DGPU_SC(2); DGPU_SC(3); DGPU_SC(4); DGPU_SC(5); DGPU_SC(6); DGPU_SC(7); DGPU_SC(8);
 #undef DGPU_SC
         default:
             set_error("stable_partition: %d modes unsupported", p.N);
             return DGPU_ERR_ARG;
     }
+    if (rc == DGPU_OK && rec) cs->replay = true;
+    return rc;
 }
 
 // The kept-table slot of LSD pass k of the running PingPong step's fiber

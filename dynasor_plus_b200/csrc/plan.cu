@@ -195,6 +195,8 @@ Plan::~Plan() {
             for (PartCacheSlot& c : per_kind) {
                 dev_free(c.off);
                 dev_free(c.base);
+                dev_free(c.lp);
+                dev_free(c.dst);
             }
     dev_free(err_flag);
     dev_free(part_ctr);
@@ -409,6 +411,7 @@ static int plan_init(Plan& p, int N, uint64_t nnz, const uint32_t* dims, const d
     if (const char* e = std::getenv("DGPU_OVERLAP")) p.overlap = std::atoi(e);
     if (const char* e = std::getenv("DGPU_PART_CACHE")) p.part_cache = std::atoi(e) != 0 ? 1 : 0;
     if (const char* e = std::getenv("DGPU_PART_CACHE_CHECK")) p.part_cache_check = std::atoi(e) != 0 ? 1 : 0;
+    if (const char* e = std::getenv("DGPU_PART_REPLAY")) p.part_replay = std::atoi(e) != 0 ? 1 : 0;
     for (int n = 0; n < N; ++n) p.dims[n] = dims[n];
     return DGPU_OK;
 }

@@ -41,17 +41,21 @@ def _slab_equal(p, o):
     return np.array_equal(pv, v) and all(np.array_equal(a, b) for a, b in zip(pix, ix))
 
 
+@pytest.mark.parametrize("replay", ["1", "0"])
 @pytest.mark.parametrize("digit", ["8", "2"])
 @pytest.mark.parametrize("fiber", [True, False])
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_sweeps_with_kept_tables_match_oracle(bindings, monkeypatch, case, fiber, digit):
+def test_sweeps_with_kept_tables_match_oracle(bindings, monkeypatch, case, fiber, digit, replay):
     """Four sweeps with the kept tables checked on the device: every slab
-    equals the oracle's.  Digit width 2 gives fiber sorts of more LSD
-    passes than the tables kept per sort (the later passes recompute)."""
+    equals the oracle's, with the passes replayed from their recordings
+    (replay "1", the default) or ranked on the kept tables ("0").  Digit
+    width 2 gives fiber sorts of more LSD passes than the tables kept per
+    sort (the later passes recompute)."""
     import dynasor_plus_b200 as d
     dims, nnz, T, R, seed, kind = CASES[case]
     monkeypatch.setenv("DGPU_PART_CACHE_CHECK", "1")
     monkeypatch.setenv("DGPU_FIBER_DIGIT_BITS", digit)
+    monkeypatch.setenv("DGPU_PART_REPLAY", replay)
     dims, vals, idx = _tensor(kind, dims, nnz, seed)
     N = len(dims)
     o = bindings.Oracle(dims, vals, idx, T)
