@@ -651,13 +651,18 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 
 // Replay of a recorded pass: the window list in order, grid-strided (the
 // destinations are recorded, so windows are independent).  Per window each
-// thread loads its elements and stores them at their recorded staging slots
-// (a 16-byte record when N <= 3, else one word per column), then writes
-// staged slot i to its recorded destination: the same bucket-ordered runs
-// the ranked scatter writes, without its ranking, counters and prefixes.
-constexpr int kReplayThreads = 256;
+// thread loads its elements, their recorded staging slots and the recorded
+// destinations of the slots it will write (all before the barrier, so one
+// memory latency per window), stores the elements at their slots (a 16-byte
+// record when N <= 3, else one word per column), then writes staged slot i
+// to its destination: the bucket-ordered runs of the ranked scatter,
+// without its ranking, counters and prefixes.  512 threads of <= 40
+// registers, 3 CTAs per SM: the kernel waits on its loads, so it is built
+// for warps in flight.
+constexpr int kReplayThreads = 512;
+constexpr int kReplayMinBlocks = 3;
 template <int N, int W>
-__global__ void __launch_bounds__(kReplayThreads)
+__global__ void __launch_bounds__(kReplayThreads, kReplayMinBlocks)
 k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
               const uint4* __restrict__ wins, uint32_t nwin, const uint16_t* __restrict__ lp,
               const uint32_t* __restrict__ dst, uint32_t total, int* __restrict__ err)
@@ -668,15 +673,17 @@ k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabO
     for (uint32_t w = blockIdx.x; w < nwin; w += gridDim.x) {
         const uint4 d = wins[w];                  // {src, list offset, count, -}
         const uint32_t cnt = min(d.z, (uint32_t)W);
-        uint32_t slot[U];
+        uint32_t slot[U], dest[U];
         float val[U];
         uint32_t id[U][N];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t j = u * kReplayThreads + threadIdx.x;
             slot[u] = 0xffffffffu;
+            dest[u] = 0xffffffffu;
             if (j < cnt) {
                 slot[u] = lp[d.y + j];
+                dest[u] = dst[d.y + j];
                 val[u] = in.vals[d.x + j];
 #pragma unroll
                 for (int m = 0; m < N; ++m) id[u][m] = in.idx[m][d.x + j];
@@ -702,7 +709,7 @@ k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabO
         for (int u = 0; u < U; ++u) {
             const uint32_t i = u * kReplayThreads + threadIdx.x;
             if (i >= cnt) break;
-            const uint32_t g = dst[d.y + i];
+            const uint32_t g = dest[u];
             if (g >= total) { atomicOr(err, kErrPartRange); continue; }
             if constexpr (kRec) {
                 const uint4 r = reinterpret_cast<const uint4*>(sm)[i];
@@ -1086,8 +1093,10 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
     const double row_bytes = 4.0 + 4.0 * p.N;
     const double elem = (double)L.total;
     if (hit && cs->replay) {
+        // algorithmic bytes: the records read and written (the recorded
+        // slots and destinations, 6 bytes per element, are overhead)
         LaunchTimer t(p, p.part_fiber ? KK_FIB_SCATTER : KK_PART_SCATTER,
-                      elem * (2.0 * row_bytes + 6.0));
+                      elem * 2.0 * row_bytes);
         switch (p.N) {
 #define DGPU_RP(NN) case NN: return launch_replay<NN>(p, in, out, L, *cs)
             DGPU_RP(2); DGPU_RP(3); DGPU_RP(4); DGPU_RP(5); DGPU_RP(6); DGPU_RP(7); DGPU_RP(8);
