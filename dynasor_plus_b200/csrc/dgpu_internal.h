@@ -103,6 +103,7 @@ struct PartList {
     uint4*    wins = nullptr;
     uint32_t  nwin = 0;
     uint32_t* tile_pre = nullptr;
+    uint32_t* tile_wb = nullptr;  // each tile's first window
     uint64_t  total = 0;          // elements listed
 };
 
@@ -124,12 +125,14 @@ struct PartCacheSlot {
     int             key_mode = -1, shift = -1;
     uint32_t        mask = 0, nb = 0;
     bool            valid = false;
-    // the pass recorded element by element (list order): each element's
-    // slot in its window's bucket-ordered staging, and each staged slot's
-    // destination; a pass with a recording is replayed without ranking
-    uint16_t*       lp = nullptr;
-    uint32_t*       dst = nullptr;
-    size_t          rec_cap = 0;               // elements of lp / dst
+    // the pass recorded: for each slot of a window's bucket-ordered staging
+    // (list order), the window index of the element staged there, and per
+    // window and bucket the destination of the window's slot 0 of that
+    // bucket (slot i of bucket b goes to tab[window][b] + i); a pass with a
+    // recording is replayed without ranking
+    uint16_t*       inv = nullptr;
+    uint32_t*       tab = nullptr;
+    size_t          inv_cap = 0, tab_cap = 0;  // entries allocated
     bool            replay = false;
 };
 

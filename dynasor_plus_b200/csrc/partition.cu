@@ -380,8 +380,8 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                 const uint32_t* __restrict__ off, const uint32_t* __restrict__ base,
                 int key_mode, int shift, uint32_t mask, uint32_t nb, uint32_t total,
                 uint32_t* __restrict__ queue, int* __restrict__ err,
-                const uint32_t* __restrict__ tile_pre, uint16_t* __restrict__ rec_lp,
-                uint32_t* __restrict__ rec_dst)
+                const uint32_t* __restrict__ tile_pre, const uint32_t* __restrict__ tile_wb,
+                uint16_t* __restrict__ rec_inv, uint32_t* __restrict__ rec_tab)
 {
     constexpr int S = W / kScatThreads;           // steps per warp per window
     constexpr int PW = W / kScatWarps;            // elements per warp per window
@@ -465,6 +465,12 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
             if (!mbar_wait(bark(kw), park(kw))) {
                 fail = 1;
                 atomicOr(err, kErrPartWait);
+            }
+            // REC: the window's list offset and index
+            uint32_t ro = 0, wid = 0;
+            if constexpr (REC) {
+                ro = tile_pre[t] + w0;
+                wid = tile_wb[t] + w0 / (uint32_t)W;
             }
             // a. load the window's elements and rank them per warp
             uint32_t key[S], rk[S];
@@ -572,22 +578,21 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                         const uint32_t cur = cursor[b];
                         wbase[b] = pre;
                         wdst[b] = cur - pre;
+                        if constexpr (REC) rec_tab[(size_t)wid * nb + b] = cur - pre;
                         cursor[b] = cur + tot[u];
                         pre += tot[u];
                     }
                 }
             }
             __syncthreads();       // (3)
-            // c. stage in bucket order (REC: each element's slot is recorded
-            //    at its list-order position)
-            uint32_t ro = 0;
-            if constexpr (REC) ro = tile_pre[t] + w0;
+            // c. stage in bucket order (REC: for each slot, the window index
+            //    of the element staged there)
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 if (key[s] == 0xffffffffu) continue;
                 const uint32_t lp = wbase[key[s]] + wc[wc_slot(key[s], warp)] + rk[s];
                 if (lp >= cnt) { atomicOr(err, kErrPartRange); continue; }
-                if constexpr (REC) rec_lp[ro + warp * PW + s * 32 + lane] = (uint16_t)lp;
+                if constexpr (REC) rec_inv[ro + lp] = (uint16_t)(warp * PW + s * 32 + lane);
                 if constexpr (kRec) {
                     uint32_t r[4] = {__float_as_uint(val[s]), 0u, 0u, 0u};
 #pragma unroll
@@ -615,7 +620,6 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                     const uint32_t kb = part_key(kv, shift, mask);
                     const uint32_t d = kb < nb ? wdst[kb] + i : total;
                     if (d >= total) { atomicOr(err, kErrPartRange); continue; }
-                    if constexpr (REC) rec_dst[ro + i] = d;
                     out.vals[d] = __uint_as_float(rv[0]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = rv[m + 1];
@@ -623,7 +627,6 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
                     const uint32_t kb = part_key(bk[(size_t)(key_mode + 1) * BW + i], shift, mask);
                     const uint32_t d = kb < nb ? wdst[kb] + i : total;
                     if (d >= total) { atomicOr(err, kErrPartRange); continue; }
-                    if constexpr (REC) rec_dst[ro + i] = d;
                     out.vals[d] = __uint_as_float(bk[i]);
 #pragma unroll
                     for (int m = 0; m < N; ++m) out.idx[m][d] = bk[(size_t)(m + 1) * BW + i];
@@ -651,57 +654,60 @@ k_chunk_scatter(const __grid_constant__ SlabPtrs in, const __grid_constant__ Sla
 
 // Replay of a recorded pass: the window list in order, grid-strided (the
 // destinations are recorded, so windows are independent).  Per window each
-// thread loads its elements, their recorded staging slots and the recorded
-// destinations of the slots it will write (all before the barrier, so one
-// memory latency per window), stores the elements at their slots (a 16-byte
-// record when N <= 3, else one word per column), then writes staged slot i
-// to its destination: the bucket-ordered runs of the ranked scatter,
-// without its ranking, counters and prefixes.  512 threads of <= 40
-// registers, 3 CTAs per SM: the kernel waits on its loads, so it is built
-// for warps in flight.
+// thread loads its elements (input order) and the recorded source element
+// of each slot it will write, and the CTA the window's bucket table -- all
+// before the barrier, so one memory latency per window; the elements are
+// stored in shared memory in input order (a 16-byte record when N <= 3, else
+// one word per column); then slot i takes element inv[i] and goes to
+// tab[b] + i (b from its key): the bucket-ordered runs of the ranked
+// scatter, without its ranking, counters and prefixes.  512 threads of
+// <= 40 registers, 3 CTAs per SM: the kernel waits on its loads, so it is
+// built for warps in flight.
 constexpr int kReplayThreads = 512;
 constexpr int kReplayMinBlocks = 3;
 template <int N, int W>
 __global__ void __launch_bounds__(kReplayThreads, kReplayMinBlocks)
 k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabOut out,
-              const uint4* __restrict__ wins, uint32_t nwin, const uint16_t* __restrict__ lp,
-              const uint32_t* __restrict__ dst, uint32_t total, int* __restrict__ err)
+              const uint4* __restrict__ wins, uint32_t nwin, const uint16_t* __restrict__ inv,
+              const uint32_t* __restrict__ tab, int key_mode, int shift, uint32_t mask,
+              uint32_t nb, uint32_t total, int* __restrict__ err)
 {
     constexpr int U = W / kReplayThreads;         // elements per thread per window
     constexpr bool kRec = (N + 1 <= 4);
-    extern __shared__ __align__(16) uint32_t sm[];   // [W] records or [N+1][W] columns
+    constexpr int C = kRec ? 4 : N + 1;
+    extern __shared__ __align__(16) uint32_t sm[];   // [W] records or [N+1][W] columns, then [nb]
+    uint32_t* stab = sm + (size_t)C * W;
     for (uint32_t w = blockIdx.x; w < nwin; w += gridDim.x) {
         const uint4 d = wins[w];                  // {src, list offset, count, -}
         const uint32_t cnt = min(d.z, (uint32_t)W);
-        uint32_t slot[U], dest[U];
+        uint32_t src[U];
         float val[U];
         uint32_t id[U][N];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t j = u * kReplayThreads + threadIdx.x;
-            slot[u] = 0xffffffffu;
-            dest[u] = 0xffffffffu;
+            src[u] = 0xffffffffu;
             if (j < cnt) {
-                slot[u] = lp[d.y + j];
-                dest[u] = dst[d.y + j];
+                src[u] = inv[d.y + j];
                 val[u] = in.vals[d.x + j];
 #pragma unroll
                 for (int m = 0; m < N; ++m) id[u][m] = in.idx[m][d.x + j];
             }
         }
+        for (uint32_t b = threadIdx.x; b < nb; b += kReplayThreads) stab[b] = tab[(size_t)w * nb + b];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (slot[u] == 0xffffffffu) continue;
-            if (slot[u] >= cnt) { atomicOr(err, kErrPartRange); continue; }
+            const uint32_t j = u * kReplayThreads + threadIdx.x;
+            if (j >= cnt) break;
             if constexpr (kRec) {
                 uint32_t r[4] = {__float_as_uint(val[u]), 0u, 0u, 0u};
 #pragma unroll
                 for (int m = 0; m < N; ++m) r[m + 1] = id[u][m];
-                reinterpret_cast<uint4*>(sm)[slot[u]] = make_uint4(r[0], r[1], r[2], r[3]);
+                reinterpret_cast<uint4*>(sm)[j] = make_uint4(r[0], r[1], r[2], r[3]);
             } else {
-                sm[slot[u]] = __float_as_uint(val[u]);
+                sm[j] = __float_as_uint(val[u]);
 #pragma unroll
-                for (int m = 0; m < N; ++m) sm[(size_t)(m + 1) * W + slot[u]] = id[u][m];
+                for (int m = 0; m < N; ++m) sm[(size_t)(m + 1) * W + j] = id[u][m];
             }
         }
         __syncthreads();
@@ -709,18 +715,25 @@ k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabO
         for (int u = 0; u < U; ++u) {
             const uint32_t i = u * kReplayThreads + threadIdx.x;
             if (i >= cnt) break;
-            const uint32_t g = dest[u];
-            if (g >= total) { atomicOr(err, kErrPartRange); continue; }
+            const uint32_t e = src[u];
+            if (e >= cnt) { atomicOr(err, kErrPartRange); continue; }
             if constexpr (kRec) {
-                const uint4 r = reinterpret_cast<const uint4*>(sm)[i];
+                const uint4 r = reinterpret_cast<const uint4*>(sm)[e];
                 const uint32_t rv[4] = {r.x, r.y, r.z, r.w};
+                const uint32_t kv = key_mode == 0 ? r.y : (key_mode == 1 ? r.z : r.w);
+                const uint32_t kb = part_key(kv, shift, mask);
+                const uint32_t g = kb < nb ? stab[kb] + i : total;
+                if (g >= total) { atomicOr(err, kErrPartRange); continue; }
                 out.vals[g] = __uint_as_float(rv[0]);
 #pragma unroll
                 for (int m = 0; m < N; ++m) out.idx[m][g] = rv[m + 1];
             } else {
-                out.vals[g] = __uint_as_float(sm[i]);
+                const uint32_t kb = part_key(sm[(size_t)(key_mode + 1) * W + e], shift, mask);
+                const uint32_t g = kb < nb ? stab[kb] + i : total;
+                if (g >= total) { atomicOr(err, kErrPartRange); continue; }
+                out.vals[g] = __uint_as_float(sm[e]);
 #pragma unroll
-                for (int m = 0; m < N; ++m) out.idx[m][g] = sm[(size_t)(m + 1) * W + i];
+                for (int m = 0; m < N; ++m) out.idx[m][g] = sm[(size_t)(m + 1) * W + e];
             }
         }
         __syncthreads();                          // staging reused by the next window
@@ -728,8 +741,8 @@ k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabO
 }
 
 template <int N>
-constexpr size_t replay_smem() {
-    return (N + 1 <= 4 ? 4 : N + 1) * (size_t)scatter_window<N>() * sizeof(uint32_t);
+size_t replay_smem(uint32_t nb) {
+    return ((N + 1 <= 4 ? 4 : N + 1) * (size_t)scatter_window<N>() + nb) * sizeof(uint32_t);
 }
 
 template <int N>
@@ -797,7 +810,7 @@ int launch_scatter(Plan& p, const Slab& in, const Slab& out, const PartList& L, 
     kern<<<grid, kScatThreads, smem, p.stream>>>(
         slab_in(in, p.N), slab_out(out, p.N), L.tiles, L.chunks, L.order, L.nchunks, off,
         base, key_mode, key_shift, key_mask, nb, (uint32_t)p.nnz, p.part_ctr, p.err_flag,
-        L.tile_pre, rec ? rec->lp : nullptr, rec ? rec->dst : nullptr);
+        L.tile_pre, L.tile_wb, rec ? rec->inv : nullptr, rec ? rec->tab : nullptr);
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
 }
@@ -807,15 +820,15 @@ int launch_replay(Plan& p, const Slab& in, const Slab& out, const PartList& L,
                   const PartCacheSlot& cs)
 {
     constexpr int W = scatter_window<N>();
-    constexpr size_t smem = replay_smem<N>();
+    const size_t smem = replay_smem<N>(cs.nb);
     auto* kern = k_part_replay<N, W>;
     DGPU_TRY(ensure_smem_limit(kern, smem, p.device));
     int per_sm = 0;
     DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kReplayThreads, smem));
     const uint32_t grid = std::max(1u, std::min(L.nwin, (uint32_t)(std::max(1, per_sm) * p.sms)));
     kern<<<grid, kReplayThreads, smem, p.stream>>>(slab_in(in, p.N), slab_out(out, p.N), L.wins,
-                                                   L.nwin, cs.lp, cs.dst, (uint32_t)p.nnz,
-                                                   p.err_flag);
+                                                   L.nwin, cs.inv, cs.tab, cs.key_mode, cs.shift,
+                                                   cs.mask, cs.nb, (uint32_t)p.nnz, p.err_flag);
     DGPU_CUDA(cudaGetLastError());
     return DGPU_OK;
 }
@@ -834,6 +847,7 @@ void free_partlist(PartList& l) {
     dev_free(l.order);
     dev_free(l.wins);
     dev_free(l.tile_pre);
+    dev_free(l.tile_wb);
     l = PartList{};
 }
 
@@ -902,11 +916,12 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     // the scatter's windows (W-element pieces of each tile) and tile offsets
     // in list order: the layout of a recorded pass
     const uint32_t W = scatter_window_host(p.N);
-    std::vector<uint32_t> pre(tiles.size());
+    std::vector<uint32_t> pre(tiles.size()), wb(tiles.size());
     std::vector<uint4> wins;
     uint64_t acc = 0;
     for (size_t t = 0; t < tiles.size(); ++t) {
         pre[t] = (uint32_t)acc;
+        wb[t] = (uint32_t)wins.size();
         for (uint32_t w0 = 0; w0 < tiles[t].count; w0 += W)
             wins.push_back(make_uint4(tiles[t].begin + w0, (uint32_t)acc + w0,
                                       std::min(W, tiles[t].count - w0), 0u));
@@ -932,6 +947,10 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     DGPU_TRY(dev_alloc(p, (void**)&out.order, std::max<size_t>(1, ch.size()) * sizeof(uint32_t)));
     DGPU_TRY(dev_alloc(p, (void**)&out.wins, std::max<size_t>(1, wins.size()) * sizeof(uint4)));
     DGPU_TRY(dev_alloc(p, (void**)&out.tile_pre, std::max<size_t>(1, pre.size()) * sizeof(uint32_t)));
+    DGPU_TRY(dev_alloc(p, (void**)&out.tile_wb, std::max<size_t>(1, wb.size()) * sizeof(uint32_t)));
+    if (!wb.empty())
+        DGPU_CUDA(cudaMemcpyAsync(out.tile_wb, wb.data(), wb.size() * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice, p.stream));
     if (!wins.empty())
         DGPU_CUDA(cudaMemcpyAsync(out.wins, wins.data(), wins.size() * sizeof(uint4),
                                   cudaMemcpyHostToDevice, p.stream));
@@ -950,30 +969,32 @@ int build_partlist(Plan& p, const std::vector<Tile>& tiles, const std::vector<ui
     return DGPU_OK;
 }
 
-// Recording buffers of a slot (one 2-byte slot and one 4-byte destination
-// per listed element), grown only while the device keeps at least a quarter
-// of its memory free; a slot without them runs its ranked scatter on the
-// kept tables.
-static int reserve_recording(Plan& p, const PartList& L, PartCacheSlot& cs) {
-    if (cs.rec_cap >= L.total) return DGPU_OK;
-    dev_free(cs.lp);
-    dev_free(cs.dst);
-    cs.lp = nullptr;
-    cs.dst = nullptr;
-    cs.rec_cap = 0;
+// Recording buffers of a slot (a 2-byte source element per listed slot and
+// a destination per window and bucket), grown only while the device keeps
+// at least a quarter of its memory free; a slot without them runs its
+// ranked scatter on the kept tables.
+static int reserve_recording(Plan& p, const PartList& L, uint32_t nb, PartCacheSlot& cs) {
+    const size_t tab_n = (size_t)L.nwin * nb;
+    if (cs.inv_cap >= L.total && cs.tab_cap >= tab_n) return DGPU_OK;
+    dev_free(cs.inv);
+    dev_free(cs.tab);
+    cs.inv = nullptr;
+    cs.tab = nullptr;
+    cs.inv_cap = cs.tab_cap = 0;
     size_t free_b = 0, total_b = 0;
     DGPU_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t need = (size_t)L.total * (sizeof(uint16_t) + sizeof(uint32_t)) + 512;
+    const size_t need = (size_t)L.total * sizeof(uint16_t) + tab_n * sizeof(uint32_t) + 512;
     if (free_b < need || free_b - need < total_b / 4) return DGPU_OK;
-    if (dev_alloc(p, (void**)&cs.lp, (size_t)L.total * sizeof(uint16_t)) != DGPU_OK ||
-        dev_alloc(p, (void**)&cs.dst, (size_t)L.total * sizeof(uint32_t)) != DGPU_OK) {
-        dev_free(cs.lp);
-        dev_free(cs.dst);
-        cs.lp = nullptr;
-        cs.dst = nullptr;
+    if (dev_alloc(p, (void**)&cs.inv, (size_t)L.total * sizeof(uint16_t)) != DGPU_OK ||
+        dev_alloc(p, (void**)&cs.tab, tab_n * sizeof(uint32_t)) != DGPU_OK) {
+        dev_free(cs.inv);
+        dev_free(cs.tab);
+        cs.inv = nullptr;
+        cs.tab = nullptr;
         return DGPU_OK;                          // no recording: not an error
     }
-    cs.rec_cap = L.total;
+    cs.inv_cap = L.total;
+    cs.tab_cap = tab_n;
     return DGPU_OK;
 }
 
@@ -1086,8 +1107,8 @@ int stable_partition(Plan& p, const Slab& in, const PartList& L, int key_mode, i
         // a PingPong pass whose tables are not kept for the next sweep
         if (p.pc_mode >= 0 && !(cs && cs->valid)) ++p.pc_uncached;
         if (filled && p.part_replay) {
-            DGPU_TRY(reserve_recording(p, L, *cs));
-            if (cs->rec_cap >= L.total) rec = cs;
+            DGPU_TRY(reserve_recording(p, L, nb, *cs));
+            if (cs->inv_cap >= L.total && cs->tab_cap >= (size_t)L.nwin * nb) rec = cs;
         }
     }
     const double row_bytes = 4.0 + 4.0 * p.N;

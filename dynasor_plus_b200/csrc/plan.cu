@@ -195,8 +195,8 @@ Plan::~Plan() {
             for (PartCacheSlot& c : per_kind) {
                 dev_free(c.off);
                 dev_free(c.base);
-                dev_free(c.lp);
-                dev_free(c.dst);
+                dev_free(c.inv);
+                dev_free(c.tab);
             }
     dev_free(err_flag);
     dev_free(part_ctr);
