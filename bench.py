@@ -59,15 +59,17 @@ RANK = 32
 METRIC = "MTTKRP GNNZ/s (nnz per full 3-mode sweep with device remap)"
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch,
-# measured by ncu on this workload at its full size (64,659,576 nnz, the
-# timed sweep of `bench.py --steps 1 --warmup 1`; one-pass metrics):
-# profiles/dram_traffic_zipf1.1_64.7M.md.  Averages over the sweep's launches
-# of each kind; scaled by nnz only when the bench runs another size.
+# measured by ncu on this workload at its full size (64,659,576 nnz; one-pass
+# metrics): profiles/k_part_replay_zipf1.1_64.7M.md (the partition passes of a
+# sweep past the slab's first cycle, replayed) and
+# profiles/dram_traffic_zipf1.1_64.7M.md (the MTTKRP).  Averages over one
+# sweep's launches of each kind; scaled by nnz only when the bench runs
+# another size.
 NCU_NNZ = 64_659_576
 NCU_DRAM_BYTES_PER_LAUNCH = {
-    "part_scatter": 2_117_256_619,     # k_chunk_scatter, the 3 remap passes
-    "fiber_scatter": 2_152_501_589,    # k_chunk_scatter, the 6 fiber-sort passes
-    "mttkrp": 3_014_740_139,           # k_mttkrp_rowrun, 3 modes (2.38 / 3.19 / 3.48 GB)
+    "part_scatter": 2_242_111_147,     # k_part_replay, the 3 remap passes
+    "fiber_scatter": 2_242_156_331,    # k_part_replay, the 6 fiber-sort passes
+    "mttkrp": 3_014_740_139,           # k_mttkrp_rowrun, 3 modes (2.37 / 3.19 / 3.47 GB)
 }
 
 

@@ -225,7 +225,12 @@ struct Plan {
     cudaStream_t ovl_stream = nullptr;          // PingPong: MTTKRP beside the remap
     cudaEvent_t  ovl_fork = nullptr, ovl_join = nullptr, ovl_tail = nullptr;
     bool         ovl_pending = false;           // work after ovl_tail's record not yet joined
-    int          overlap = 1;                   // 0: MTTKRP then remap on the plan stream
+    // 0: MTTKRP then remap on the plan stream; 1: MTTKRP launched first on a
+    // second stream beside the remap; 2 (default): the remap's first pass
+    // launched first at remap_ctas CTAs per SM, the MTTKRP beside it
+    int          overlap = 2;
+    int          remap_ctas = 1;                // overlap 2: remap CTAs per SM beside the MTTKRP
+    int          replay_cap = 0;                // > 0: replayed passes run at most this many CTAs per SM
     Slab         slab[kMaxModes];               // 2 for PingPong, N for NCopy
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for
@@ -439,8 +444,11 @@ void free_partlist(PartList& l);
 // partition pass per least-significant digit (later passes in slab order),
 // ping-ponging between slab[a] and slab[b]; *result receives the slab index
 // that holds the sorted data.
+// Passes [k0, k1) only (k1 < 0: to the last) -- the remap split around the
+// MTTKRP launched beside it.
 int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first,
-                         int key_mode, int key_shift, uint64_t key_limit, int* result);
+                         int key_mode, int key_shift, uint64_t key_limit, int* result,
+                         int k0 = 0, int k1 = -1);
 
 // MTTKRP of mode n over the tiles of the slab `in` into p.Yhat[n].
 int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles);

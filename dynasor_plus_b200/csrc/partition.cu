@@ -825,6 +825,7 @@ int launch_replay(Plan& p, const Slab& in, const Slab& out, const PartList& L,
     DGPU_TRY(ensure_smem_limit(kern, smem, p.device));
     int per_sm = 0;
     DGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kReplayThreads, smem));
+    if (p.replay_cap > 0) per_sm = std::min(per_sm, p.replay_cap);   // beside the MTTKRP
     const uint32_t grid = std::max(1u, std::min(L.nwin, (uint32_t)(std::max(1, per_sm) * p.sms)));
     kern<<<grid, kReplayThreads, smem, p.stream>>>(slab_in(in, p.N), slab_out(out, p.N), L.wins,
                                                    L.nwin, cs.inv, cs.tab, cs.key_mode, cs.shift,
@@ -1151,7 +1152,7 @@ static PartCacheSlot* cache_slot(Plan& p, int kind, int k) {
 }
 
 int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first, int key_mode,
-                         int key_shift, uint64_t key_limit, int* result)
+                         int key_shift, uint64_t key_limit, int* result, int k0, int k1)
 {
     int bits = 0;
     while (bits < 32 && ((uint64_t)1 << bits) < key_limit) ++bits;
@@ -1161,7 +1162,8 @@ int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first, int key_m
     if (passes < 1) passes = 1;
     const int dbits = (bits + passes - 1) / passes;
     int src = a, dst = b;
-    for (int k = 0; k < passes; ++k) {
+    const int kend = k1 < 0 ? passes : std::min(passes, k1);
+    for (int k = k0; k < kend; ++k) {
         const int sh = key_shift + k * dbits;
         uint32_t nb, mask;
         if (passes == 1) {

@@ -409,6 +409,7 @@ static int plan_init(Plan& p, int N, uint64_t nnz, const uint32_t* dims, const d
     if (const char* e = std::getenv("DGPU_MTTKRP_KERNEL")) p.mttkrp_kernel = std::atoi(e) == 1 ? 1 : 0;
     if (const char* e = std::getenv("DGPU_RANK_TILE")) p.rank_tile = std::atoi(e);
     if (const char* e = std::getenv("DGPU_OVERLAP")) p.overlap = std::atoi(e);
+    if (const char* e = std::getenv("DGPU_REMAP_CTAS")) p.remap_ctas = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("DGPU_PART_CACHE")) p.part_cache = std::atoi(e) != 0 ? 1 : 0;
     if (const char* e = std::getenv("DGPU_PART_CACHE_CHECK")) p.part_cache_check = std::atoi(e) != 0 ? 1 : 0;
     if (const char* e = std::getenv("DGPU_PART_REPLAY")) p.part_replay = std::atoi(e) != 0 ? 1 : 0;
@@ -900,7 +901,7 @@ static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwai
     // into the slab the MTTKRP is reading
     const int digit = std::max(1, std::min(kDigitBits, p.sort_digit_bits));
     const bool one_pass = (uint64_t)p.K[nm] <= ((uint64_t)1 << digit);
-    if (p.overlap == 0 || p.timing || !one_pass) {
+    if (p.overlap == 0 || p.timing || (!one_pass && p.overlap != 2)) {
         DGPU_TRY(pingpong_drain(p));
         DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
         if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
@@ -909,13 +910,17 @@ static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwai
     } else {
         // The MTTKRP and the remap both only read the live slab (the remap
         // writes the other one), so the MTTKRP runs on ovl_stream beside the
-        // remap on the plan stream.  The MTTKRP is launched first; the
-        // remap's CTAs start as its last CTAs drain (each kernel fills the
-        // SMs' registers, so that tail is the overlap; measured 9.72 -> 9.61
-        // ms per sweep on the 64.7M-nonzero tensor).  The plan stream waits
-        // for the MTTKRP only (the next mode's fiber sort overwrites the
-        // slab it read); `after` stays on ovl_stream, beside the remap and
-        // the next fiber sort, until pingpong_drain.
+        // remap on the plan stream.  Each kernel alone fills the SMs'
+        // registers.  Overlap 1 launches the MTTKRP first and the remap's
+        // CTAs start as its last CTAs drain (measured 9.72 -> 9.61 ms per
+        // sweep on the 64.7M-nonzero tensor, ranked passes).  Overlap 2
+        // launches the remap's first pass first at remap_ctas CTAs per SM
+        // when it is replayed, so the MTTKRP fills the rest of every SM
+        // beside it (7.64 -> 7.38 ms, replayed passes).  The plan stream
+        // waits for the MTTKRP before any pass that rewrites the slab it
+        // reads (the next mode's fiber sort, a later LSD pass of the remap);
+        // `after` stays on ovl_stream, beside the remap and the next fiber
+        // sort, until pingpong_drain.
         if (!p.ovl_stream) {
             DGPU_CUDA(cudaStreamCreateWithFlags(&p.ovl_stream, cudaStreamNonBlocking));
             DGPU_CUDA(cudaEventCreateWithFlags(&p.ovl_fork, cudaEventDisableTiming));
@@ -928,8 +933,19 @@ static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwai
         struct Restore {
             Plan& p;
             cudaStream_t s;
-            ~Restore() { p.stream = s; }
+            ~Restore() { p.stream = s; p.replay_cap = 0; }
         } restore{p, main};
+        // DGPU_OVERLAP=2: the remap's first pass is launched first with at
+        // most remap_ctas CTAs per SM (when it is replayed), so the MTTKRP
+        // launched next beside it fills the rest of every SM; later passes
+        // rewrite the slab the MTTKRP reads and wait for it
+        int r0 = 0;
+        if (p.overlap == 2) {
+            p.replay_cap = p.remap_ctas;
+            DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm],
+                                          &r0, 0, 1));
+            p.replay_cap = 0;
+        }
         p.stream = p.ovl_stream;
         DGPU_TRY(launch_mttkrp(p, n, p.slab[p.cur], p.tiles_d[n], (uint32_t)p.tiles_h[n].size()));
         if (after_mttkrp) DGPU_CUDA(cudaEventRecord(after_mttkrp, p.stream));
@@ -940,8 +956,14 @@ static int mode_pingpong_impl(Plan& p, int n, const cudaEvent_t* waits, int nwai
             p.ovl_pending = true;
         }
         p.stream = main;
-        DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm], &r));
-        DGPU_CUDA(cudaStreamWaitEvent(main, p.ovl_join, 0));
+        if (p.overlap == 2) {
+            DGPU_CUDA(cudaStreamWaitEvent(main, p.ovl_join, 0));
+            DGPU_TRY(stable_sort_pingpong(p, r0, 1 - r0, p.proc[n], nm, p.shift[nm], p.K[nm], &r, 1));
+        } else {
+            DGPU_TRY(stable_sort_pingpong(p, p.cur, 1 - p.cur, p.proc[n], nm, p.shift[nm], p.K[nm],
+                                          &r));
+            DGPU_CUDA(cudaStreamWaitEvent(main, p.ovl_join, 0));
+        }
     }
     p.cur = r;
     p.next_mode = nm;

@@ -32,11 +32,12 @@ def _assert_slab(p, v_ref, i_ref, what):
         assert np.array_equal(ix[k], i_ref[k]), (what, k)
 
 
-@pytest.mark.parametrize("overlap", ["1", "0"])
+@pytest.mark.parametrize("overlap", ["1", "0", "2"])
 @pytest.mark.parametrize("name", SWEEP_CASES)
 def test_golden_sweeps(name, overlap, monkeypatch):
     # overlap "1": each PingPong MTTKRP runs on a second stream beside the
-    # remap (the default); "0": both on the plan stream, one after the other
+    # remap (the default); "0": both on the plan stream, one after the other;
+    # "2": the remap's first pass launched first, the MTTKRP beside it
     monkeypatch.setenv("DGPU_OVERLAP", overlap)
     g = load_golden(name)
     dims = g["dims"]

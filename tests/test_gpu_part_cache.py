@@ -133,3 +133,34 @@ def test_kept_tables_follow_autotuned_knobs(bindings):
     sweep()
     sweep()
     p.close()
+
+
+@pytest.mark.parametrize("ctas", ["1", "3"])
+@pytest.mark.parametrize("case", ["zipf3", "lsd"])
+def test_remap_first_overlap_matches_oracle(bindings, monkeypatch, case, ctas):
+    """DGPU_OVERLAP=2: each mode's first remap pass (replayed from the third
+    sweep on, at most `ctas` CTAs per SM) is launched before the MTTKRP on
+    the second stream, and a later LSD pass of the remap waits for the
+    MTTKRP; the slabs equal the oracle's and Yhat its FP64 MTTKRP."""
+    import dynasor_plus_b200 as d
+    dims, nnz, T, R, seed, kind = CASES[case]
+    monkeypatch.setenv("DGPU_OVERLAP", "2")
+    monkeypatch.setenv("DGPU_REMAP_CTAS", ctas)
+    dims, vals, idx = _tensor(kind, dims, nnz, seed)
+    o = bindings.Oracle(dims, vals, idx, T)
+    p = d.Plan(dims, vals, idx, threads=T, rank=R)
+    Y = bindings.uniform_factors(seed, dims, R)
+    for n in range(3):
+        p.set_factor(n, Y[n])
+    for s in range(4):
+        for n in range(3):
+            if o.kclass[n] == 2:
+                o.fiber_sort(n)
+            v, ix = o.slab()
+            y64 = bindings.mttkrp_f64(v, ix, n, Y, R, int(dims[n]))
+            o.remap(n)
+            p.process(n)
+            assert _slab_equal(p, o), f"sweep {s} mode {n}"
+            assert rel_fro(p.yhat(n)[:, :R], y64[:, :R]) <= 1e-5, (s, n)
+    p.close()
+
