@@ -96,6 +96,8 @@ def parse():
                     help="skip the BF16-gather CP-ALS block (4-mode rank-64 tensor)")
     ap.add_argument("--bf16-draws", type=int, default=200_000_000,
                     help="coordinate draws of the 4-mode tensor of the BF16 block")
+    ap.add_argument("--bf16-sweeps", type=int, default=2,
+                    help="timed plain sweeps per plan of the BF16 block (launched from the host)")
     ap.add_argument("--no-cpopt", action="store_true",
                     help="skip the CP-OPT forward / gradient block (20M-nonzero tensor)")
     ap.add_argument("--no-batched", action="store_true",
@@ -213,7 +215,8 @@ def bf16_block(device, stream, args):
     noise, rank 64, Gauss-Seidel, both layouts.  Each timed run follows a
     warm-up run on the same plan; fits of the two precisions are compared
     iteration by iteration (their distance from FP64 CP-ALS is checked in
-    tests/test_gpu_configs.py)."""
+    tests/test_gpu_configs.py).  Each plan then times plain sweeps, every
+    mode gathering in its precision (`--bf16-sweeps`)."""
     import torch
     import dynasor_plus_b200 as d
     from dynasor_plus_b200 import synth
@@ -224,6 +227,7 @@ def bf16_block(device, stream, args):
                        f"{len(vals)} nnz, rank 64, GS, FP64 solve", "iters": it}
     for layout in ("ncopy", "pingpong"):
         res = {}
+        sweep_ms = {}
         for prec in ("fp32", "bf16"):
             p = d.Plan(dims, vals, idx, threads=args.threads, rank=64, layout=layout,
                        precision=prec, device=device)
@@ -231,12 +235,25 @@ def bf16_block(device, stream, args):
             p.cpals(max_iters=it, tol=0.0, seed=42)            # warm-up run
             r = p.cpals(max_iters=it, tol=0.0, seed=42)
             res[prec] = r
+            # plain sweeps launched from the host (every mode gathers in this
+            # precision): one untimed, then args.bf16_sweeps timed
+            if args.bf16_sweeps > 0:
+                p.sweep()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(args.bf16_sweeps):
+                    p.sweep()
+                e1.record(stream)
+                e1.synchronize()
+                sweep_ms[prec] = e0.elapsed_time(e1) / args.bf16_sweeps
             p.close()
             torch.cuda.synchronize()
         f32, b16 = res["fp32"], res["bf16"]
         ips = {k: v["iters_done"] / v["total_time_s"] for k, v in res.items()}
         out[layout] = {"fp32_iter_per_s": ips["fp32"], "bf16_iter_per_s": ips["bf16"],
                        "bf16_speedup": ips["bf16"] / ips["fp32"],
+                       "fp32_sweep_ms": sweep_ms.get("fp32"), "bf16_sweep_ms": sweep_ms.get("bf16"),
                        "fp32_final_fit": f32["final_fit"], "bf16_final_fit": b16["final_fit"],
                        "max_abs_fit_diff_bf16_vs_fp32": float(np.max(np.abs(
                            b16["fit_history"] - f32["fit_history"])))}
