@@ -72,6 +72,25 @@ __device__ __forceinline__ float gather1(const FacPtrs& F, int w, uint32_t row, 
     else return __ldg(F.Y[w] + (size_t)row * RP + c);
 }
 
+// Products of the two BF16 values in each half of words a and b, exact in
+// FP32 (two 8-bit significands), by sm_100's mixed-precision FMA
+// (fma.rn.f32.bf16: BF16 multiplicands, FP32 addend and result) with a zero
+// addend: no conversion instructions.  .x = low halves, .y = high halves.
+__device__ __forceinline__ float2 bf16x2_products(uint32_t a, uint32_t b) {
+    float lo, hi;
+    asm("{\n\t.reg .b16 a0, a1, b0, b1;\n\t"
+        "mov.b32 {a0, a1}, %2;\n\t"
+        "mov.b32 {b0, b1}, %3;\n\t"
+        "fma.rn.f32.bf16 %0, a0, b0, 0f00000000;\n\t"
+        "fma.rn.f32.bf16 %1, a1, b1, 0f00000000;\n\t}"
+        : "=f"(lo), "=f"(hi) : "r"(a), "r"(b));
+    return make_float2(lo, hi);
+}
+// BF16 half h (0 low, 1 high) of word w as FP32 (exact).
+__device__ __forceinline__ float bf16_half(uint32_t w, int h) {
+    return __uint_as_float(h ? (w & 0xffff0000u) : (w << 16));
+}
+
 // ===========================================================================
 //  ROWRUN
 // ===========================================================================
@@ -120,6 +139,13 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     (void)w0_rt;
     const int wl = TN >= 0 ? (N == 2 ? -1 : (TN == N - 1 ? N - 2 : N - 1)) : wl_rt;
     constexpr int U = RunBatch<N, V, BF>::U;
+    // BF16 rows with the target pinned (3 and 4 modes): rows kept as raw
+    // BF16 pairs; the first two gathered modes (MA < MB) multiply by the
+    // mixed-precision FMA, a third (MC, 4 modes) is widened
+    constexpr bool kMix = BF && TN >= 0 && V == 1 && (N == 3 || N == 4);
+    constexpr int MA = TN == 0 ? 1 : 0;
+    constexpr int MB = (MA + 1 == TN) ? MA + 2 : MA + 1;
+    constexpr int MC = N == 4 ? 6 - TN - MA - MB : 0;
     constexpr int NG = 32 / G;                    // groups per warp
     constexpr int CH = G >= 16 ? G : ((1 + N + 3) / 4 * 4 > 8 ? 8 : 16);  // staged per group
     constexpr int LPE = CH / G;                   // nonzeros loaded per lane per chunk
@@ -191,7 +217,8 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
         for (int e0 = 0; e0 < cnt; e0 += U) {
             float val[U];
             uint32_t row[U];
-            float y[U][N][V][4];
+            float y[U][kMix ? 1 : N][V][4];
+            uint32_t yr[U][kMix ? N : 1][2];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int e = e0 + u;
@@ -205,16 +232,29 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
                 row[u] = 0u;
 #pragma unroll
                 for (int w = 0; w < N; ++w) row[u] = (w == n) ? s[1 + w] : row[u];
+                if constexpr (kMix) {
 #pragma unroll
-                for (int w = 0; w < N; ++w) {
-                    const uint32_t id = s[1 + w];
+                    for (int w = 0; w < N; ++w) {
+                        yr[u][w][0] = yr[u][w][1] = 0u;
+                        if (w != TN) {
+                            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(
+                                                        F.Yb[w] + (size_t)s[1 + w] * ld) + gl);
+                            yr[u][w][0] = raw.x;
+                            yr[u][w][1] = raw.y;
+                        }
+                    }
+                } else {
 #pragma unroll
-                    for (int v = 0; v < V; ++v) {
-                        const int c4 = gl + v * G;
-                        float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
-                        y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
-                        y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
+                    for (int w = 0; w < N; ++w) {
+                        const uint32_t id = s[1 + w];
+#pragma unroll
+                        for (int v = 0; v < V; ++v) {
+                            const int c4 = gl + v * G;
+                            float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (w != n && (V == 1 || c4 < C4)) g4 = gather4<BF>(F, w, id, ld, c4);
+                            y[u][w][v][0] = g4.x; y[u][w][v][1] = g4.y;
+                            y[u][w][v][2] = g4.z; y[u][w][v][3] = g4.w;
+                        }
                     }
                 }
             }
@@ -242,6 +282,23 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
                             first_run = false;
                         }
                         cur = row[u];
+                    }
+                    if constexpr (kMix) {
+                        // rows MA x MB exact in FP32, times the value, times
+                        // row MC (4 modes) in the accumulating FMA
+                        const float2 p0 = bf16x2_products(yr[u][MA][0], yr[u][MB][0]);
+                        const float2 p1 = bf16x2_products(yr[u][MA][1], yr[u][MB][1]);
+                        const float t[4] = {p0.x, p0.y, p1.x, p1.y};
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            if constexpr (N == 3) {
+                                acc[0][q] = __fmaf_rn(val[u], t[q], acc[0][q]);
+                            } else {
+                                const float yc = bf16_half(yr[u][MC][q >> 1], q & 1);
+                                acc[0][q] = __fmaf_rn(val[u] * t[q], yc, acc[0][q]);
+                            }
+                        }
+                        continue;
                     }
                     // non-target modes in increasing order: the first starts
                     // the product (w0), the middle ones multiply, the last
