@@ -110,6 +110,8 @@ struct RunBatch {
     // and on the 4-mode rank-64 tensor (NCopy CP-ALS iterations/s):
     //   FP32 4/2 34.3, 3/2 32.8, 3/3 29.8, 5/1 36.0, 6/1 33.2 (spills);
     //   BF16 4/2 31.2, 4/4 22.4, 3/3 28.8, 5/1 35.8, 6/1 36.9
+    // and, BF16 rows as raw pairs with mixed-precision products (MTTKRP ms
+    // per sweep, 3-mode / 4-mode): 6/1 2.71 / 20.65, 4/2 3.15 / 25.58
     static constexpr bool kQuad = (N == 4 && V == 1);
     static constexpr int U = kWork <= 2 ? 1 : (kQuad ? 1 : (kWork <= 4 ? 2 : 1));
     static constexpr int kMinBlocks = kWork <= 2 ? 6 : (kQuad ? (BF ? 6 : 5) : (N <= 4 ? 4 : 2));
