@@ -155,7 +155,14 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     // Group slot areas are CH*SW + 4 words apart so the NG groups' 16-byte
     // slot reads of one instruction land in distinct banks.
     constexpr int GS = CH * SW + 4;
-    __shared__ __align__(16) uint32_t slots[kRunWarps * NG * GS];
+    // kAsync: the next chunk's metadata streams into a second slot buffer
+    // with cp.async instead of through registers, which frees the registers
+    // (and the spill) of the 3-mode FP32 kernel: sweep 7.39 -> 7.25 ms on
+    // the 64.7M-nonzero tensor.  Measured slower for BF16 rows (2.70 ->
+    // 2.78 ms) and 4 modes (27.3 -> 27.7 ms), and at 8 CTAs per SM, where
+    // no room is left for the remap beside the MTTKRP.
+    constexpr bool kAsync = N == 3 && !BF && 2u * kRunWarps * NG * GS * 4u <= 48u * 1024u;
+    __shared__ __align__(16) uint32_t slots[kAsync ? 2 : 1][kRunWarps * NG * GS];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / G, gl = lane % G;
@@ -177,7 +184,8 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     const uint32_t gb = min(we, wb + grp * per_g);
     const uint32_t ge = min(we, gb + per_g);
     const uint32_t nchunks = (per_g + CH - 1) / CH;          // warp-uniform
-    uint32_t* gs = slots + (warp * NG + grp) * GS;
+    uint32_t* const gs0 = slots[0] + (warp * NG + grp) * GS;
+    uint32_t* const gs1 = slots[kAsync ? 1 : 0] + (warp * NG + grp) * GS;
 
     float acc[V][4];
 #pragma unroll
@@ -187,33 +195,62 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
     uint32_t cur = 0xffffffffu;
     bool first_run = true;                 // the run at the start of this group's slice
 
-    // prefetch registers for one chunk
-    uint32_t pf[LPE][SW];
+    // the next chunk's metadata: in registers (stored to the slot buffer
+    // when its chunk starts), or, kAsync, copied by cp.async into the other
+    // slot buffer (no registers held for it)
+    uint32_t pf[kAsync ? 1 : LPE][SW];
     auto prefetch = [&](uint32_t ch) {
 #pragma unroll
         for (int k = 0; k < LPE; ++k) {
             const uint32_t e = gb + ch * CH + gl + k * G;
             const uint32_t p = tl.begin + (e < ge ? e : gb);
-            // the slab is read once per sweep: streaming loads (evict first)
-            // keep L2 for the factor rows the gathers reuse
-            pf[k][0] = __float_as_uint(__ldcs(in.vals + p));
+            if constexpr (kAsync) {
+                uint32_t* dst = ((ch & 1u) ? gs1 : gs0) + (gl + k * G) * SW;
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;"
+                             :: "r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(in.vals + p)
+                             : "memory");
 #pragma unroll
-            for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldcs(in.idx[w] + p);
+                for (int w = 0; w < N; ++w)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;"
+                                 :: "r"((uint32_t)__cvta_generic_to_shared(dst + 1 + w)),
+                                    "l"(in.idx[w] + p)
+                                 : "memory");
+            } else {
+                // the slab is read once per sweep: streaming loads (evict
+                // first) keep L2 for the factor rows the gathers reuse
+                pf[k][0] = __float_as_uint(__ldcs(in.vals + p));
 #pragma unroll
-            for (int f = 1 + N; f < SW; ++f) pf[k][f] = 0u;
+                for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldcs(in.idx[w] + p);
+#pragma unroll
+                for (int f = 1 + N; f < SW; ++f) pf[k][f] = 0u;
+            }
         }
+        if constexpr (kAsync) asm volatile("cp.async.commit_group;" ::: "memory");
     };
     if (nchunks) prefetch(0);
 
     for (uint32_t ch = 0; ch < nchunks; ++ch) {
+        const uint32_t* gs;
+        if constexpr (kAsync) {
+            if (ch + 1 < nchunks) {
+                prefetch(ch + 1);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+            __syncwarp();
+            gs = (ch & 1u) ? gs1 : gs0;
+        } else {
 #pragma unroll
-        for (int k = 0; k < LPE; ++k)
+            for (int k = 0; k < LPE; ++k)
 #pragma unroll
-            for (int f = 0; f < SW; f += 4)
-                *reinterpret_cast<uint4*>(gs + (gl + k * G) * SW + f) =
-                    make_uint4(pf[k][f], pf[k][f + 1], pf[k][f + 2], pf[k][f + 3]);
-        __syncwarp();
-        if (ch + 1 < nchunks) prefetch(ch + 1);
+                for (int f = 0; f < SW; f += 4)
+                    *reinterpret_cast<uint4*>(gs0 + (gl + k * G) * SW + f) =
+                        make_uint4(pf[k][f], pf[k][f + 1], pf[k][f + 2], pf[k][f + 3]);
+            __syncwarp();
+            if (ch + 1 < nchunks) prefetch(ch + 1);
+            gs = gs0;
+        }
         const uint32_t base = gb + ch * CH;
         const int cnt = base < ge ? (int)min((uint32_t)CH, ge - base) : 0;
         for (int e0 = 0; e0 < cnt; e0 += U) {
