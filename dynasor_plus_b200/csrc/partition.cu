@@ -675,7 +675,7 @@ k_part_replay(const __grid_constant__ SlabPtrs in, const __grid_constant__ SlabO
     constexpr int U = W / kReplayThreads;         // elements per thread per window
     constexpr bool kRec = (N + 1 <= 4);
     constexpr int C = kRec ? 4 : N + 1;
-    extern __shared__ __align__(16) uint32_t sm[];   // [W] records or [N+1][W] columns, then [nb]
+    extern __shared__ __align__(128) uint32_t sm[];  // [W] records or [N+1][W] columns, then [nb]
     uint32_t* stab = sm + (size_t)C * W;
     for (uint32_t w = blockIdx.x; w < nwin; w += gridDim.x) {
         const uint4 d = wins[w];                  // {src, list offset, count, -}
