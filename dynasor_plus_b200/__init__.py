@@ -429,15 +429,27 @@ class Plan:
         check(lib().dgpu_tensor_norm_sq(self._h, C.byref(out)))
         return out.value
 
-    def model_values(self):
-        """CP model at every nonzero of the current slab (FP32)."""
-        out = np.zeros(self.nnz, np.float32)
+    def model_values(self, out=None):
+        """CP model at every nonzero of the current slab (FP32).  `out`: a
+        C-contiguous float32 array of nnz entries to write into (reused
+        across calls, it saves allocating and first touching the pages)."""
+        if out is None:
+            out = np.empty(self.nnz, np.float32)
+        elif out.dtype != np.float32 or out.size != self.nnz or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of nnz entries")
         check(lib().dgpu_model_values(self._h, out.ctypes.data))
         return out
 
-    def cpopt_gradient(self):
-        """d(0.5*||X - M||^2)/dY[n] for every n (list of I_n x Rp float32)."""
-        out = [np.zeros((int(self.dims[n]), self.Rp), np.float32) for n in range(self.N)]
+    def cpopt_gradient(self, out=None):
+        """d(0.5*||X - M||^2)/dY[n] for every n (list of I_n x Rp float32).
+        `out`: such a list to write into (reused across calls)."""
+        if out is None:
+            out = [np.empty((int(self.dims[n]), self.Rp), np.float32) for n in range(self.N)]
+        else:
+            for n, o in enumerate(out):
+                if (o.dtype != np.float32 or o.shape != (int(self.dims[n]), self.Rp)
+                        or not o.flags.c_contiguous):
+                    raise ValueError(f"out[{n}] must be a C-contiguous float32 I_n x Rp array")
         check(lib().dgpu_cpopt_gradient(self._h, _ptrs(out)))
         return out
 

@@ -1825,11 +1825,16 @@ int cpopt_gradient(Plan& p, float* const* grad_host) {
         k_grad_rows<<<grid_for((size_t)p.dims[n] * p.Rp), kLaThreads, sm, p.stream>>>(
             p.Y[n], p.Yhat[n], p.dims[n], p.R, p.Rp, L.Wd, g);
         DGPU_CUDA(cudaGetLastError());
-        DGPU_CUDA(cudaMemcpyAsync(grad_host[n], g, (size_t)p.dims[n] * p.Rp * sizeof(float),
-                                  cudaMemcpyDeviceToHost, p.stream));
         off += (size_t)p.dims[n] * p.Rp;
     }
-    return sync_checked(p);
+    // to the caller's (possibly pageable) buffers through pinned chunks
+    off = 0;
+    for (int n = 0; n < p.N; ++n) {
+        const size_t cnt = (size_t)p.dims[n] * p.Rp;
+        DGPU_TRY(copy_to_host_staged(p, grad_host[n], p.grad_buf + off, cnt * sizeof(float)));
+        off += cnt;
+    }
+    return DGPU_OK;
 }
 
 }  // namespace dgpu

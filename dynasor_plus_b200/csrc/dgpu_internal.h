@@ -270,6 +270,12 @@ struct Plan {
     bool         gather_fp32_all = false;       // every mode gathers FP32 (gradient path)
     float*       grad_buf = nullptr;            // CP-OPT gradients of all modes
     size_t       grad_cap = 0;                  // floats in grad_buf
+    float*       model_buf = nullptr;           // CP-OPT model values at the nonzeros
+    size_t       model_cap = 0;                 // floats in model_buf
+    // two pinned chunks that copies to pageable host memory go through
+    void*        stage_host[2] = {nullptr, nullptr};
+    size_t       stage_cap = 0;                 // bytes of each chunk
+    cudaEvent_t  stage_ev[2] = {nullptr, nullptr};
     uint32_t*    part_cnt = nullptr;            // [chunks x buckets] counts
     uint32_t*    part_off = nullptr;            // [chunks x buckets] in-segment prefixes
     size_t       part_cap = 0;                  // entries of each
@@ -465,6 +471,10 @@ int launch_mttkrp_gather(Plan& p, int n, const Slab& in, const Tile* tiles, uint
 
 // FP32 -> BF16 factor mirror.
 int launch_to_bf16(Plan& p, int n);
+// bytes from device memory to host memory the caller may not have pinned:
+// chunk k+1 is copied to one of the plan's two pinned chunks while the host
+// moves chunk k out of the other; waits for the plan stream (extras.cu)
+int copy_to_host_staged(Plan& p, void* host, const void* dev, size_t bytes);
 
 // Dense CP-ALS pieces.
 int cp_tensor_norm(Plan& p, const float* vals, double* out);

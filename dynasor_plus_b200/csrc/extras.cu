@@ -12,6 +12,8 @@
 // ============================================================================
 #include "dgpu_internal.h"
 
+#include <cstring>
+
 #include <algorithm>
 #include <vector>
 
@@ -230,6 +232,49 @@ int launch_model_values(Plan& p, float* out) {
     return by_modes(p.N, [&](auto NC) { return model_values_n<decltype(NC)::value>(p, src, out); });
 }
 
+// Bytes from device memory to host memory the caller may not have pinned,
+// through the plan's two pinned chunks: the GPU copies chunk k+1 while the
+// host moves chunk k out (pageable copies otherwise run at a few GB/s).
+int copy_to_host_staged(Plan& p, void* host, const void* dev, size_t bytes) {
+    constexpr size_t kChunk = (size_t)8 << 20;
+    if (bytes == 0) return DGPU_OK;
+    if (p.stage_cap < kChunk) {
+        for (int k = 0; k < 2; ++k) {
+            if (p.stage_host[k]) cudaFreeHost(p.stage_host[k]);
+            p.stage_host[k] = nullptr;
+        }
+        p.stage_cap = 0;
+        for (int k = 0; k < 2; ++k) {
+            if (cudaMallocHost(&p.stage_host[k], kChunk) != cudaSuccess) {
+                cudaGetLastError();
+                set_error("copy to host: pinned staging of %zu bytes failed", kChunk);
+                return DGPU_ERR_NOMEM;
+            }
+            if (!p.stage_ev[k])
+                DGPU_CUDA(cudaEventCreateWithFlags(&p.stage_ev[k], cudaEventDisableTiming));
+        }
+        p.stage_cap = kChunk;
+    }
+    const char* src = static_cast<const char*>(dev);
+    char* dst = static_cast<char*>(host);
+    const size_t nchunks = (bytes + kChunk - 1) / kChunk;
+    auto issue = [&](size_t k) -> int {
+        const size_t off = k * kChunk, len = std::min(kChunk, bytes - off);
+        DGPU_CUDA(cudaMemcpyAsync(p.stage_host[k & 1], src + off, len, cudaMemcpyDeviceToHost,
+                                  p.stream));
+        DGPU_CUDA(cudaEventRecord(p.stage_ev[k & 1], p.stream));
+        return DGPU_OK;
+    };
+    DGPU_TRY(issue(0));
+    for (size_t k = 0; k < nchunks; ++k) {
+        if (k + 1 < nchunks) DGPU_TRY(issue(k + 1));      // the other chunk, while this one drains
+        DGPU_CUDA(cudaEventSynchronize(p.stage_ev[k & 1]));
+        const size_t off = k * kChunk, len = std::min(kChunk, bytes - off);
+        std::memcpy(dst + off, p.stage_host[k & 1], len);
+    }
+    return sync_checked(p);
+}
+
 }  // namespace dgpu
 
 using namespace dgpu;
@@ -247,20 +292,16 @@ int dgpu_model_values(dgpu_plan* plan, float* model_host) {
     Plan* p = reinterpret_cast<Plan*>(plan);
     if (!p || !model_host) { set_error("dgpu_model_values: null argument"); return DGPU_ERR_ARG; }
     DGPU_CUDA(cudaSetDevice(p->device));
-    float* d = nullptr;
-    DGPU_TRY(dev_alloc(*p, (void**)&d, p->nnz * sizeof(float)));
-    int rc = launch_model_values(*p, d);
-    if (rc == DGPU_OK) {
-        if (cudaMemcpyAsync(model_host, d, p->nnz * sizeof(float), cudaMemcpyDeviceToHost,
-                            p->stream) != cudaSuccess ||
-            cudaStreamSynchronize(p->stream) != cudaSuccess) {
-            set_error("dgpu_model_values: copy-back failed");
-            rc = DGPU_ERR_CUDA;
-        }
+    // the device buffer is kept on the plan for later calls
+    if (p->model_cap < p->nnz) {
+        dev_free(p->model_buf);
+        p->model_buf = nullptr;
+        p->model_cap = 0;
+        DGPU_TRY(dev_alloc(*p, (void**)&p->model_buf, p->nnz * sizeof(float)));
+        p->model_cap = p->nnz;
     }
-    dev_free(d);
-    p->device_bytes -= p->nnz * sizeof(float);
-    return rc;
+    DGPU_TRY(launch_model_values(*p, p->model_buf));
+    return copy_to_host_staged(*p, model_host, p->model_buf, p->nnz * sizeof(float));
 }
 
 int dgpu_cpopt_gradient(dgpu_plan* plan, float* const* grad_host) {

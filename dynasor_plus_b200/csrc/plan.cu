@@ -208,6 +208,11 @@ Plan::~Plan() {
     if (cp_loop_exec) cudaGraphExecDestroy(cp_loop_exec);
     if (cp_batch_exec) cudaGraphExecDestroy(cp_batch_exec);
     dev_free(grad_buf);
+    dev_free(model_buf);
+    for (int k = 0; k < 2; ++k) {
+        if (stage_host[k]) cudaFreeHost(stage_host[k]);
+        if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
+    }
     dev_free(cp_st);
     if (cp_fit_host) cudaFreeHost(cp_fit_host);
     for (auto e : cp_ev) cudaEventDestroy(e);

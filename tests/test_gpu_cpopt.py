@@ -142,3 +142,37 @@ def test_model_values_vs_oracle(bindings):
     v, ix = p.slab()
     m64 = bindings.model_values(ix, Y, R)
     assert np.max(np.abs(m - m64)) < 1e-5 * max(1.0, np.max(np.abs(m64)))
+
+
+def test_outputs_into_caller_buffers_match_fresh_ones():
+    """model_values / cpopt_gradient written into the caller's arrays (the
+    copies go through the plan's pinned chunks, here across several 8 MB
+    chunks) equal freshly allocated results, on two calls in a row; a
+    buffer of the wrong shape or type is refused."""
+    import dynasor_plus_b200 as d
+    from dynasor_plus_b200 import synth
+    dims, vals, idx = synth.uniform((60000, 50000, 400), 3_000_000, seed=5, values="normal")
+    rng = np.random.default_rng(6)
+    R = 32
+    # NCopy: the slab order (and so the order of the model values) stays
+    # put across the gradient's mode passes
+    p = d.Plan(dims, vals, idx, threads=4, rank=R, layout="ncopy")
+    for n in range(3):
+        y = np.zeros((int(dims[n]), p.Rp), np.float32)
+        y[:, :R] = rng.normal(0, 0.1, (int(dims[n]), R))
+        p.set_factor(n, y)
+    m0 = p.model_values()
+    g0 = p.cpopt_gradient()
+    mo = np.full(p.nnz, np.nan, np.float32)
+    go = [np.full_like(g, np.nan) for g in g0]
+    for _ in range(2):
+        assert p.model_values(out=mo) is mo
+        assert np.array_equal(mo, m0)
+        assert p.cpopt_gradient(out=go) is go
+        for a, b in zip(go, g0):
+            assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+    with pytest.raises(ValueError):
+        p.model_values(out=np.zeros(p.nnz - 1, np.float32))
+    with pytest.raises(ValueError):
+        p.cpopt_gradient(out=[g.astype(np.float64) for g in g0])
+    p.close()
