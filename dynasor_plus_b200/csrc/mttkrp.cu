@@ -112,6 +112,7 @@ struct RunBatch {
     //   BF16 4/2 31.2, 4/4 22.4, 3/3 28.8, 5/1 35.8, 6/1 36.9
     // and, BF16 rows as raw pairs with mixed-precision products (MTTKRP ms
     // per sweep, 3-mode / 4-mode): 6/1 2.71 / 20.65, 4/2 3.15 / 25.58
+    // and, FP32 3-mode with cp.async metadata: 6/1 3.30, 5/2 3.44
     static constexpr bool kQuad = (N == 4 && V == 1);
     static constexpr int U = kWork <= 2 ? 1 : (kQuad ? 1 : (kWork <= 4 ? 2 : 1));
     static constexpr int kMinBlocks = kWork <= 2 ? 6 : (kQuad ? (BF ? 6 : 5) : (N <= 4 ? 4 : 2));
