@@ -219,6 +219,8 @@ k_mttkrp_rowrun(const __grid_constant__ SlabPtrs in, const Tile* __restrict__ ti
             } else {
                 // the slab is read once per sweep: streaming loads (evict
                 // first) keep L2 for the factor rows the gathers reuse
+                // (plain __ldg measured: 3-mode BF16 2.71 -> 2.83 ms per
+                // sweep, 4-mode within 0.5%)
                 pf[k][0] = __float_as_uint(__ldcs(in.vals + p));
 #pragma unroll
                 for (int w = 0; w < N; ++w) pf[k][1 + w] = __ldcs(in.idx[w] + p);
