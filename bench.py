@@ -44,6 +44,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -76,7 +77,8 @@ NCU_DRAM_BYTES_PER_LAUNCH = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 150 on the GPU, so the timed region spans several 200 ms clock samples; 20 reference sweeps)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--threads", type=int, default=16,
@@ -103,7 +105,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched blocks (16 restarts; 32 tensors)")
     ap.add_argument("--json-out", default=None)
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.impl == "reference" else 150
+    return args
 
 
 def peaks():
@@ -115,8 +120,47 @@ def peaks():
         return 6650.0, "fallback"
 
 
+CLOCK_REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+
+def summarize_clocks(lines, t0=None, t1=None):
+    """Median SM clock, max clock and active throttle reasons of the
+    nvidia-smi samples `lines` ((monotonic time, csv line) pairs) taken
+    inside the timed region [t0, t1]; when the region is shorter than the
+    sampling period and holds none, the first sample after t0 stands in."""
+    parsed = []
+    for t, line in lines:
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm, smax = float(f[1]), float(f[2])
+        except ValueError:
+            continue
+        rs = {nm for k, nm in enumerate(CLOCK_REASONS) if f[5 + k].lower().startswith("active")}
+        parsed.append((t, sm, smax, rs))
+    if not parsed:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+    sel = parsed
+    if t0 is not None and t1 is not None:
+        sel = [x for x in parsed if t0 <= x[0] <= t1]
+        if not sel:
+            sel = [x for x in parsed if x[0] >= t0][:1] or parsed[-1:]
+    reasons = set()
+    for x in sel:
+        reasons |= x[3]
+    out = {"sm_mhz": statistics.median(x[1] for x in sel),
+           "sm_max_mhz": max(x[2] for x in sel),
+           "reasons": sorted(reasons), "samples": len(sel), "samples_total": len(parsed)}
+    if t0 is not None and t1 is not None:
+        out["timed_region_s"] = round(t1 - t0, 3)
+    return out
+
+
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms, read by a
+    thread as they arrive; `start` returns once the first sample is in, and
+    `begin`/`end` mark the timed region the summary keeps."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -125,15 +169,34 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
+        self.thread = None
+        self.lines = []
+        self.t0 = self.t1 = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.monotonic(), line))
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, bufsize=1)
         except Exception:
             self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        deadline = time.monotonic() + 5.0
+        while not self.lines and self.proc.poll() is None and time.monotonic() < deadline:
+            time.sleep(0.01)
+
+    def begin(self):
+        self.t0 = time.monotonic()
+
+    def end(self):
+        self.t1 = time.monotonic()
 
     def stop(self):
         if not self.proc:
@@ -141,28 +204,12 @@ class ClockSampler:
         time.sleep(0.25)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-            out = ""
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if f[5 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        return summarize_clocks(list(self.lines), self.t0, self.t1)
 
 
 def make_workload(args, device="cuda"):
@@ -516,11 +563,13 @@ def main():
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clk.begin()
     e0.record(stream)
     for _ in range(args.steps):
         plan.sweep()
     e1.record(stream)
     e1.synchronize()
+    clk.end()
     torch.cuda.synchronize()
     barrier()
     clocks = clk.stop()
