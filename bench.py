@@ -70,7 +70,7 @@ NCU_NNZ = 64_659_576
 NCU_DRAM_BYTES_PER_LAUNCH = {
     "part_scatter": 2_242_111_147,     # k_part_replay, the 3 remap passes
     "fiber_scatter": 2_242_156_331,    # k_part_replay, the 6 fiber-sort passes
-    "mttkrp": 3_014_740_139,           # k_mttkrp_rowrun, 3 modes (2.37 / 3.19 / 3.47 GB)
+    "mttkrp": 2_089_282_219,           # k_mttkrp_rowrun, 3 modes (1.60 / 2.14 / 2.53 GB)
 }
 
 
