@@ -177,6 +177,10 @@ class OwnerComputesCpals:
             local_mttkrp = EngineMttkrp(dims, vals, idx, self.blocks, self.me, rank, threads,
                                         self.device)
         self.mttkrp = local_mttkrp
+        # gloo collectives take host tensors: device tensors are staged
+        # through host memory for them (NCCL takes device tensors as they are)
+        self.stage = (self.ws > 1 and self.device.type == "cuda"
+                      and dist.get_backend(group) == "gloo")
         lo, hi = self.blocks[self.N - 1][self.me], self.blocks[self.N - 1][self.me + 1]
         mine = (idx[self.N - 1] >= lo) & (idx[self.N - 1] < hi)
         v = vals[mine].astype(np.float64)
@@ -185,7 +189,12 @@ class OwnerComputesCpals:
     # -- collectives -----------------------------------------------------
     def _allreduce(self, t):
         if self.ws > 1:
-            self.dist.all_reduce(t, group=self.group)
+            if self.stage and t.is_cuda:
+                h = t.cpu()
+                self.dist.all_reduce(h, group=self.group)
+                t.copy_(h)
+            else:
+                self.dist.all_reduce(t, group=self.group)
         return t
 
     def _sum(self, x: float) -> float:
@@ -201,8 +210,13 @@ class OwnerComputesCpals:
         mx = max(b[k + 1] - b[k] for k in range(self.ws))
         pad = torch.zeros((mx, self.Rp), dtype=blk.dtype, device=blk.device)
         pad[:blk.shape[0]] = blk
-        out = torch.empty((self.ws * mx, self.Rp), dtype=blk.dtype, device=blk.device)
-        self.dist.all_gather_into_tensor(out, pad, group=self.group)
+        if self.stage and pad.is_cuda:
+            out = torch.empty((self.ws * mx, self.Rp), dtype=blk.dtype)
+            self.dist.all_gather_into_tensor(out, pad.cpu(), group=self.group)
+            out = out.to(blk.device)
+        else:
+            out = torch.empty((self.ws * mx, self.Rp), dtype=blk.dtype, device=blk.device)
+            self.dist.all_gather_into_tensor(out, pad, group=self.group)
         return torch.cat([out[k * mx:k * mx + b[k + 1] - b[k]] for k in range(self.ws)])
 
     # -- the run ---------------------------------------------------------

@@ -3,8 +3,9 @@
 rank, with and without an NCCL process group, follows FP64 CP-ALS and the
 single-plan run; (2) the row blocks of two ranks are built as two sets of
 engine plans in one process, and their MTTKRP rows, put together, equal the
-FP64 MTTKRP of the whole tensor (the collectives themselves run on gloo
-ranks in tests/test_owner_computes_gloo.py)."""
+FP64 MTTKRP of the whole tensor; (3) two ranks run as two processes on this
+GPU, each with its own engine plans, over a gloo group (collectives staged
+through host memory), and follow FP64 CP-ALS."""
 from __future__ import annotations
 
 import os
@@ -76,3 +77,53 @@ def test_two_ranks_engine_rows_cover_the_mttkrp(bindings):
         assert rel_fro(rows[:, :R], y64[:, :R]) < 1e-5, n
     for r in ranks:
         r.close()
+
+
+def _proc_rank(rank, ws, port, out):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from dynasor_plus_b200 import distributed as D
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=ws,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        dims, vals, idx = _case()
+        run = D.OwnerComputesCpals(dims, vals, idx, 8, threads=8, device="cuda:0")
+        assert run.stage
+        r = run.run(max_iters=12, tol=0.0, seed=42)
+        run.close()
+        out.put((rank, r["fit_history"], [f[:, :8] for f in r["factors"]]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_processes_follow_fp64(bindings):
+    """Two ranks as two processes, each with its own engine plans on this
+    GPU and its own CUDA context; the collectives are gloo's, staged through
+    host memory (no kernel of one rank waits for the other's)."""
+    import torch.multiprocessing as mp
+    ws = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=_proc_rank, args=(r, ws, port, q)) for r in range(ws)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=300) for _ in range(ws)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    dims, vals, idx = _case()
+    fit64, Y64, _ = bindings.cpals_f64(dims, vals, idx, 8, 12, 0.0, seed=42)
+    for rank, fits, Y in res:
+        print(f"\nowner-computes, 2 processes, rank {rank}: max |fit - fp64| "
+              f"{np.max(np.abs(fits - fit64)):.2e}")
+        assert np.max(np.abs(fits - fit64)) < 1e-6
+        for n in range(3):
+            assert rel_fro(Y[n], Y64[n][:, :8]) < 1e-4, (rank, n)
+    for n in range(3):
+        assert np.array_equal(res[0][2][n], res[1][2][n])
