@@ -235,6 +235,10 @@ struct Plan {
     int          cur = 0;                       // PingPong: live slab index
     int          next_mode = 0;                 // PingPong: mode the slab is sorted for
     Tile*        tiles_d[kMaxModes] = {nullptr};   // mode n tiles, processing order
+    // the MTTKRP's CTA tiles: processing-order tiles of one shard merged
+    // in pairs for 3-mode plans (rowrun_tiles in plan.cu), else tiles_d
+    Tile*        run_tiles_d[kMaxModes] = {nullptr};
+    uint32_t     run_tiles_n[kMaxModes] = {0};
     PartList     proc[kMaxModes];               // remap of mode n (global, processing order)
     PartList     fib[kMaxModes];                // fiber sort of mode n (segmented by shard)
     PartList     ident;                         // identity order over [0, nnz) (global)
@@ -458,6 +462,7 @@ int stable_sort_pingpong(Plan& p, int a, int b, const PartList& first,
 
 // MTTKRP of mode n over the tiles of the slab `in` into p.Yhat[n].
 int launch_mttkrp(Plan& p, int n, const Slab& in, const Tile* tiles, uint32_t ntiles);
+int mttkrp_scheme(const Plan& p, int n);   // DGPU_ACCUM_ROWRUN or DGPU_ACCUM_PRIVATE
 // All-modes pass over the plan's live nonzeros (SoA slab or Morton keys).
 int launch_mttkrp_all_modes(Plan& p);
 // Values array of the live nonzeros (any order).
