@@ -70,7 +70,7 @@ NCU_NNZ = 64_659_576
 NCU_DRAM_BYTES_PER_LAUNCH = {
     "part_scatter": 2_168_673_365,     # k_part_replay, the 3 remap passes
     "fiber_scatter": 2_169_593_941,    # k_part_replay, the 6 fiber-sort passes
-    "mttkrp": 2_089_282_219,           # k_mttkrp_rowrun, 3 modes (1.60 / 2.14 / 2.53 GB)
+    "mttkrp": 2_015_217_408,           # k_mttkrp_rowrun, 3 modes (1.57 / 2.06 / 2.41 GB)
 }
 
 
