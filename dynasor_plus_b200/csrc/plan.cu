@@ -496,7 +496,9 @@ static int device_shard_counts(Plan& p, const Slab& s, std::vector<std::vector<u
 // neighbours (each flushed by an atomic) and the CTAs' start-up; measured on
 // the 3-mode rank-32 Zipf tensor, MTTKRP per sweep: 4096-nonzero CTAs 3.31 ms
 // (FP32) / 2.71 ms (BF16), 8192 3.20 / 2.55, 16384 3.31 ms FP32, and 2048
-// (a tile split in two) 3.70 ms.  The partition passes keep kTile tiles.
+// (a tile split in two) 3.70 ms.  On the 4-mode rank-64 tensor merged pairs
+// measured within 0.6% (NCopy sweep 27.3 -> 27.1 ms FP32, 20.6 ms BF16), so
+// 4-mode plans keep kTile CTAs.  The partition passes keep kTile tiles.
 constexpr uint32_t kRunTileMerge = 2;
 
 static int upload_run_tiles(Plan& p, int n) {
